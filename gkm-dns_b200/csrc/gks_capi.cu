@@ -1,0 +1,479 @@
+// C ABI of the WENO-GKS step (declarations in include/gks_b200.h).
+//
+// A context owns, per field, one device allocation of 30 * nc^3 doubles
+// (state 5, reconstruction 10, fluxes 15; the statistics reuse the flux
+// arrays as scratch), the field's descriptor in a device array, and one
+// CUDA graph holding a whole step for all fields (seven persistent launches).
+// The reference instead allocates 50 padded arrays per rank and copies the
+// whole field host<->device every step (GPUAlloc.cu:3-17, GPUupdate.cu:74-190).
+#include "../../include/gks_b200.h"
+#include "gks_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using gks::FieldDev;
+
+namespace {
+
+struct FieldHost {
+    gks_phys phys;
+    FieldDev dev;
+    double *mem = nullptr;
+    double *spl = nullptr;
+    bool uploaded = false;
+    bool have_dt = false;
+};
+
+} // namespace
+
+struct gks_ctx {
+    int nfields = 0;
+    int precision = 0;
+    int flags = 0;
+    int device = 0;
+    int nsm = 148;
+    std::vector<FieldHost> fh;
+    FieldDev *d_fields = nullptr;
+    gks::Batch batch{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraphExec_t graph = nullptr;
+    double *d_stage = nullptr;
+    size_t stage_elems = 0;
+    double *d_partial = nullptr;
+    double *d_sums = nullptr;
+    unsigned long long *d_bits = nullptr;
+    int *d_err = nullptr;
+    gks::LaunchCfg cfg[gks::K_KINDS][3];
+    std::string err;
+};
+
+namespace {
+
+int fail(gks_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(gks_ctx *c, cudaError_t e, const char *what)
+{
+    return fail(c, GKS_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                 \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+void drop_graph(gks_ctx *ctx)
+{
+    if (ctx->graph) {
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+}
+
+int check_field(gks_ctx *ctx, int f)
+{
+    if (!ctx) return GKS_EINVAL;
+    if (f < 0 || f >= ctx->nfields) return fail(ctx, GKS_EINVAL, "field index out of range");
+    return GKS_OK;
+}
+
+// Coefficients of the natural-spline slope system on nt points:
+// Thomas pivots for rows (2,1), (1,4,1)..., (1,2).
+void spline_coeffs(int nt, std::vector<double> &cp, std::vector<double> &inv)
+{
+    cp.assign(nt, 0.0);
+    inv.assign(nt, 0.0);
+    cp[0] = 0.5;
+    inv[0] = 0.5;
+    for (int p = 1; p < nt; ++p) {
+        const double b = (p == nt - 1) ? 2.0 : 4.0;
+        const double c = (p == nt - 1) ? 0.0 : 1.0;
+        const double den = b - cp[p - 1];
+        cp[p] = c / den;
+        inv[p] = 1.0 / den;
+    }
+}
+
+int ensure_stage(gks_ctx *ctx, int f)
+{
+    const size_t nt = (size_t)ctx->fh[f].phys.nc + 6;
+    const size_t need = 5 * nt * nt * nt;
+    if (ctx->stage_elems >= need) return GKS_OK;
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    ctx->d_stage = nullptr;
+    ctx->stage_elems = 0;
+    if (cudaMalloc(&ctx->d_stage, need * sizeof(double)) != cudaSuccess)
+        return fail(ctx, GKS_ENOMEM, "staging buffer allocation failed");
+    ctx->stage_elems = need;
+    return GKS_OK;
+}
+
+int push_field(gks_ctx *ctx, int f)
+{
+    CK(cudaMemcpyAsync(ctx->d_fields + f, &ctx->fh[f].dev, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GKS_OK;
+}
+
+int read_err(gks_ctx *ctx, int *word, bool clear)
+{
+    CK(cudaMemcpyAsync(word, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (clear) CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GKS_OK;
+}
+
+void choose_launch(gks_ctx *ctx)
+{
+    // persistent grids: every SM filled to its occupancy limit, no more blocks than work
+    const long long total = ctx->batch.total;
+    for (int kind = 0; kind < gks::K_KINDS; ++kind)
+        for (int dir = 0; dir < 3; ++dir) {
+            const int block = kind == gks::K_UPDATE ? 256 : 128;
+            int per_sm = 1;
+            if (gks::max_resident_blocks(kind, dir, ctx->precision, block, &per_sm) != cudaSuccess || per_sm < 1)
+                per_sm = 1;
+            long long g = (long long)ctx->nsm * per_sm;
+            const long long need = (total + block - 1) / block;
+            if (g > need) g = need;
+            if (g < 1) g = 1;
+            ctx->cfg[kind][dir].block = block;
+            ctx->cfg[kind][dir].grid = (int)g;
+        }
+}
+
+int record_step(gks_ctx *ctx)
+{
+    for (int dir = 0; dir < 3; ++dir) {
+        CK(gks::launch_recon(ctx->batch, dir, ctx->precision, ctx->cfg[gks::K_RECON][dir], ctx->stream));
+        CK(gks::launch_flux(ctx->batch, dir, ctx->precision, ctx->cfg[gks::K_FLUX][dir], ctx->stream));
+    }
+    CK(gks::launch_update(ctx->batch, ctx->cfg[gks::K_UPDATE][0], ctx->stream));
+    return GKS_OK;
+}
+
+int build_graph(gks_ctx *ctx)
+{
+    drop_graph(ctx);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = record_step(ctx);
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc != GKS_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+    const cudaError_t ei = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return cuda_fail(ctx, ei, "cudaGraphInstantiate");
+    return GKS_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *gks_last_error(const gks_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, int flags)
+{
+    if (!out || nfields < 1 || !phys) return GKS_EINVAL;
+    *out = nullptr;
+    if (precision != GKS_FP64 && precision != GKS_MIXED) return GKS_EINVAL;
+    if (flags & ~(GKS_FIX_ZSWEEP | GKS_DIRECT_ENERGY)) return GKS_EINVAL;
+    for (int f = 0; f < nfields; ++f) {
+        const gks_phys &p = phys[f];
+        if (p.nc < 4 || p.nc > 4096 || !(p.gam > 1.0) || !(p.R > 0) || !(p.T0 > 0) || !(p.mu0 >= 0) ||
+            p.K < 0 || (p.visc_law != GKS_VISC_SUTHERLAND && p.visc_law != GKS_VISC_POWER) || !(p.pr_factor > 0))
+            return GKS_EINVAL;
+    }
+    gks_ctx *ctx = new gks_ctx();
+    ctx->nfields = nfields;
+    ctx->precision = precision;
+    ctx->flags = flags;
+    auto bail = [&](int rc) {
+        gks_destroy(ctx);
+        return rc;
+    };
+    if (cudaGetDevice(&ctx->device) != cudaSuccess) return bail(GKS_ECUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) return bail(GKS_ECUDA);
+    ctx->nsm = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GKS_ECUDA);
+    ctx->own_stream = true;
+
+    ctx->fh.resize(nfields);
+    long long base = 0;
+    const double pi = std::atan(1.0) * 4.0; // param.h:14
+    for (int f = 0; f < nfields; ++f) {
+        FieldHost &h = ctx->fh[f];
+        h.phys = phys[f];
+        const gks_phys &p = phys[f];
+        const long long n = (long long)p.nc * p.nc * p.nc;
+        if (cudaMalloc(&h.mem, (size_t)30 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+        cudaMemset(h.mem, 0, (size_t)30 * n * sizeof(double));
+        FieldDev &d = h.dev;
+        memset(&d, 0, sizeof(d));
+        for (int q = 0; q < 5; ++q) d.W[q] = h.mem + q * n;
+        for (int q = 0; q < 10; ++q) d.rec[q] = h.mem + (5 + q) * n;
+        for (int q = 0; q < 15; ++q) d.F[q] = h.mem + (15 + q) * n;
+        const int nt = p.nc + 6;
+        std::vector<double> cp, inv;
+        spline_coeffs(nt, cp, inv);
+        if (cudaMalloc(&h.spl, 2 * (size_t)nt * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+        cudaMemcpy(h.spl, cp.data(), nt * sizeof(double), cudaMemcpyHostToDevice);
+        cudaMemcpy(h.spl + nt, inv.data(), nt * sizeof(double), cudaMemcpyHostToDevice);
+        d.spl_cp = h.spl;
+        d.spl_inv = h.spl + nt;
+        d.base = base;
+        d.ncell = n;
+        base += n;
+        d.nc = p.nc;
+        d.K = p.K;
+        d.visc_law = p.visc_law;
+        d.flags = flags;
+        d.dx = 2.0 * pi / p.nc; // FlowField.cpp:45
+        d.inv_dx = 1 / d.dx;
+        d.dt = 0.0;
+        d.gam = p.gam;
+        d.gm1 = p.gam - 1;
+        d.R = p.R;
+        d.cT = (p.gam - 1) / p.R;
+        d.icT = p.R / (p.gam - 1.0);
+        d.T0 = p.T0;
+        d.iT0 = 1.0 / p.T0;
+        d.mu0 = p.mu0;
+        d.visc_exp = p.visc_exp;
+        d.kA = p.pr_factor * 4.0 / (p.K + 3);
+        // spline grid of the reference's einspline call (Interpolation.cpp:10-12)
+        const double start = (0 - 3) * d.dx + 0.5 * d.dx;
+        const double end = start + (nt - 1) * d.dx;
+        d.spl_s = 3.0 / ((end - start) / (double)(nt - 1));
+    }
+    if (cudaMalloc(&ctx->d_fields, nfields * sizeof(FieldDev)) != cudaSuccess) return bail(GKS_ENOMEM);
+    for (int f = 0; f < nfields; ++f)
+        cudaMemcpy(ctx->d_fields + f, &ctx->fh[f].dev, sizeof(FieldDev), cudaMemcpyHostToDevice);
+    if (cudaMalloc(&ctx->d_partial, (size_t)148 * 32 * 24 * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+    if (cudaMalloc(&ctx->d_sums, 32 * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+    if (cudaMalloc(&ctx->d_bits, sizeof(unsigned long long)) != cudaSuccess) return bail(GKS_ENOMEM);
+    if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return bail(GKS_ENOMEM);
+    cudaMemset(ctx->d_err, 0, sizeof(int));
+    ctx->batch.fields = ctx->d_fields;
+    ctx->batch.nfields = nfields;
+    ctx->batch.total = base;
+    ctx->batch.err = ctx->d_err;
+    choose_launch(ctx);
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(GKS_ECUDA);
+    *out = ctx;
+    return GKS_OK;
+}
+
+void gks_destroy(gks_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);
+    for (FieldHost &h : ctx->fh) {
+        if (h.mem) cudaFree(h.mem);
+        if (h.spl) cudaFree(h.spl);
+    }
+    if (ctx->d_fields) cudaFree(ctx->d_fields);
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->d_partial) cudaFree(ctx->d_partial);
+    if (ctx->d_sums) cudaFree(ctx->d_sums);
+    if (ctx->d_bits) cudaFree(ctx->d_bits);
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int gks_upload(gks_ctx *ctx, int f, double *const W[5])
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!W) return fail(ctx, GKS_EINVAL, "null field pointer");
+    for (int q = 0; q < 5; ++q)
+        if (!W[q]) return fail(ctx, GKS_EINVAL, "null component pointer");
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensure_stage(ctx, f))) return rc;
+    const size_t nt = (size_t)ctx->fh[f].phys.nc + 6, Nt = nt * nt * nt;
+    for (int q = 0; q < 5; ++q)
+        CK(cudaMemcpyAsync(ctx->d_stage + q * Nt, W[q], Nt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(gks::launch_gather(ctx->fh[f].dev, ctx->d_stage, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->fh[f].uploaded = true;
+    return GKS_OK;
+}
+
+int gks_download(gks_ctx *ctx, int f, double *const W[5])
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!W) return fail(ctx, GKS_EINVAL, "null field pointer");
+    for (int q = 0; q < 5; ++q)
+        if (!W[q]) return fail(ctx, GKS_EINVAL, "null component pointer");
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensure_stage(ctx, f))) return rc;
+    const size_t nt = (size_t)ctx->fh[f].phys.nc + 6, Nt = nt * nt * nt;
+    CK(gks::launch_scatter(ctx->fh[f].dev, ctx->d_stage, ctx->stream));
+    for (int q = 0; q < 5; ++q)
+        CK(cudaMemcpyAsync(W[q], ctx->d_stage + q * Nt, Nt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GKS_OK;
+}
+
+int gks_set_dt(gks_ctx *ctx, int f, double dt)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(ctx, GKS_EINVAL, "dt must be positive and finite");
+    CK(cudaSetDevice(ctx->device));
+    ctx->fh[f].dev.dt = dt;
+    ctx->fh[f].have_dt = true;
+    return push_field(ctx, f);
+}
+
+int gks_timestep(gks_ctx *ctx, int f, double cfl, double *dt_out)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!(cfl > 0.0)) return fail(ctx, GKS_EINVAL, "cfl must be positive");
+    if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "timestep before upload");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(ctx->d_bits, 0, sizeof(unsigned long long), ctx->stream));
+    CK(gks::launch_maxwave(ctx->fh[f].dev, ctx->d_bits, ctx->stream));
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, ctx->d_bits, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double maxval;
+    memcpy(&maxval, &bits, sizeof(double));
+    if (!(maxval > 0.0) || !std::isfinite(maxval)) return fail(ctx, GKS_ENONFINITE, "max wave speed is not finite");
+    const double dt = cfl * ctx->fh[f].dev.dx / maxval; // update.cpp:1078
+    if (dt_out) *dt_out = dt;
+    return gks_set_dt(ctx, f, dt);
+}
+
+int gks_step(gks_ctx *ctx, int nsteps)
+{
+    if (!ctx) return GKS_EINVAL;
+    if (nsteps < 0) return fail(ctx, GKS_EINVAL, "negative step count");
+    for (int f = 0; f < ctx->nfields; ++f) {
+        if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "step before upload of field " + std::to_string(f));
+        if (!ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "step before dt of field " + std::to_string(f));
+    }
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->graph) {
+        int rc = build_graph(ctx);
+        if (rc) return rc;
+    }
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    return GKS_OK;
+}
+
+int gks_sync(gks_ctx *ctx)
+{
+    if (!ctx) return GKS_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    int word = 0;
+    int rc = read_err(ctx, &word, true);
+    if (rc) return rc;
+    if (word) return fail(ctx, GKS_ENONFINITE, "a step produced non-finite or non-positive density/pressure");
+    return GKS_OK;
+}
+
+int gks_check(gks_ctx *ctx)
+{
+    if (!ctx) return GKS_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    for (int f = 0; f < ctx->nfields; ++f) {
+        CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        CK(gks::launch_check(ctx->fh[f].dev, ctx->d_err, ctx->stream));
+        int word = 0;
+        int rc = read_err(ctx, &word, true);
+        if (rc) return rc;
+        if (word) return fail(ctx, GKS_ENONFINITE, "field " + std::to_string(f) + " holds non-finite or non-positive density/pressure");
+    }
+    return GKS_OK;
+}
+
+int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!out) return fail(ctx, GKS_EINVAL, "null output");
+    if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "stats before upload");
+    CK(cudaSetDevice(ctx->device));
+    const FieldDev &d = ctx->fh[f].dev;
+    CK(gks::launch_stats(d, d.F[0], ctx->d_partial, ctx->d_sums, ctx->stream));
+    double s[21];
+    CK(cudaMemcpyAsync(s, ctx->d_sums, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const gks_phys &p = ctx->fh[f].phys;
+    const double Nc = (double)d.ncell;
+    // PrintStats normalisation (update.cpp:727-776); s[0..17] are means already
+    out->tke = s[0];
+    out->diss = s[1];
+    out->sijsij = s[2];
+    out->skew[0] = s[4] / std::pow(s[3], 1.5);
+    out->skew[1] = s[7] / std::pow(s[6], 1.5);
+    out->skew[2] = s[10] / std::pow(s[9], 1.5);
+    out->kurt[0] = s[5] / (s[3] * s[3]);
+    out->kurt[1] = s[8] / (s[6] * s[6]);
+    out->kurt[2] = s[11] / (s[9] * s[9]);
+    out->prms = std::sqrt(s[18] / Nc) / (p.gam * p.p0 * p.Mt * p.Mt);
+    out->trms = std::sqrt(s[19] / Nc) / ((p.gam - 1) * p.T0 * p.Mt * p.Mt);
+    out->vrms = std::sqrt(s[20] / Nc) / (p.Mt * p.Mt / p.den0);
+    out->mach_t = std::sqrt(s[15]) / s[16];
+    out->rho_mean = s[17];
+    return GKS_OK;
+}
+
+int gks_device_fields(gks_ctx *ctx, int f, double *dW[5])
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!dW) return fail(ctx, GKS_EINVAL, "null output");
+    for (int q = 0; q < 5; ++q) dW[q] = ctx->fh[f].dev.W[q];
+    ctx->fh[f].uploaded = true; // the caller may fill the arrays in place
+    return GKS_OK;
+}
+
+int gks_set_stream(gks_ctx *ctx, void *stream)
+{
+    if (!ctx) return GKS_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    drop_graph(ctx);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+        ctx->own_stream = false;
+    } else {
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    return GKS_OK;
+}
+
+int gks_get_stream(gks_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream) return GKS_EINVAL;
+    *stream = (void *)ctx->stream;
+    return GKS_OK;
+}
+
+} // extern "C"

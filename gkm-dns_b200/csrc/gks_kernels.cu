@@ -1,0 +1,629 @@
+// Kernels of the WENO-GKS step and its diagnostics (sm_100a).
+//
+// A step is seven launches over every field of the batch: for each sweep
+// direction a reconstruction launch (WENO once per cell line and interface)
+// and a flux launch (transverse slopes from the neighbouring lines' WENO
+// states, BGK-NS flux), then the conservative update.  All launches are
+// persistent grid-stride loops over the cells of all fields, so one launch
+// covers an ensemble of fields of different sizes.  The periodic halo of the
+// reference (HaloTransfer on one rank, update.cpp:894-1054) is the index wrap
+// in `shift`.
+#include "gks_device.cuh"
+#include "gks_kernels.cuh"
+#include "../../include/gks_b200.h"
+
+#include <cuda_runtime.h>
+#include <type_traits>
+
+namespace gks {
+
+namespace {
+
+__device__ __forceinline__ int field_of(const FieldDev *f, int n, long long it)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (f[mid].base <= it) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct Cell {
+    int j, i, k, nc;
+    long long c;
+};
+
+__device__ __forceinline__ Cell decode(long long c, int nc)
+{
+    Cell x;
+    x.nc = nc;
+    x.c = c;
+    x.k = int(c % nc);
+    const long long r = c / nc;
+    x.i = int(r % nc);
+    x.j = int(r / nc);
+    return x;
+}
+
+__device__ __forceinline__ int wrap(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
+
+// Linear index of the cell displaced by (dj, di, dk), periodic.
+__device__ __forceinline__ long long shift(const Cell &x, int dj, int di, int dk)
+{
+    const int n = x.nc;
+    return ((long long)wrap(x.j + dj, n) * n + wrap(x.i + di, n)) * n + wrap(x.k + dk, n);
+}
+
+// Displacement along the sweep axis: DIR 0 = x (i), 1 = y (j), 2 = z (k).
+template <int DIR>
+__device__ __forceinline__ long long along(const Cell &x, int d)
+{
+    return DIR == 0 ? shift(x, 0, d, 0) : (DIR == 1 ? shift(x, d, 0, 0) : shift(x, 0, 0, d));
+}
+
+__device__ __forceinline__ double viscosity(const FieldDev &f, double T)
+{
+    const double x = T * f.iT0;
+    if (f.visc_law == GKS_VISC_POWER) return f.mu0 * pow(x, f.visc_exp);
+    // mu0 (T/T0)^1.5 (T0 + 110.4)/(T + 110.4), update.cpp:263
+    return f.mu0 * (x * sqrt(x)) * (f.T0 + 110.4) / (T + 110.4);
+}
+
+__device__ __forceinline__ double temperature(const double W[5], double cT)
+{
+    // (gam-1)(E/rho - |m|^2/(2 rho^2))/R, update.cpp:560
+    const double ri = __drcp_rn(W[0]);
+    return cT * (W[4] * ri - 0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * (ri * ri));
+}
+
+// ---------------------------------------------------------------------------
+// Reconstruction: Wl, Wr at the interface between cell c and its +1
+// neighbour along DIR (update.cpp:247 / GPUupdate.cu:917-977).
+// ---------------------------------------------------------------------------
+template <int DIR, int PREC>
+__global__ void __launch_bounds__(128) k_recon(Batch b)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
+        const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
+        const Cell x = decode(it - f.base, f.nc);
+        long long idx[6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) idx[a] = along<DIR>(x, a - 2);
+        double s[6][5];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s[a][q] = __ldg(f.W[q] + idx[a]);
+        const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
+        double wl[5], wr[5];
+        if (PREC == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                weno_pair<double>(s[0][q], s[1][q], s[2][q], s[3][q], s[4][q], s[5][q], kWenoEps, wl[q], wr[q]);
+            if (direct) {
+                weno_pair<double>(s[0][4], s[1][4], s[2][4], s[3][4], s[4][4], s[5][4], kWenoEps, wl[4], wr[4]);
+            } else {
+                double T[6];
+#pragma unroll
+                for (int a = 0; a < 6; ++a) T[a] = temperature(s[a], f.cT);
+                double tl, tr;
+                weno_pair<double>(T[0], T[1], T[2], T[3], T[4], T[5], kWenoEps, tl, tr);
+                // E from the reconstructed temperature (update.cpp:618-619)
+                const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
+                wl[4] = wl[0] * tl * f.icT + 0.5 * (wl[1] * wl[1] + wl[2] * wl[2] + wl[3] * wl[3]) * il;
+                wr[4] = wr[0] * tr * f.icT + 0.5 * (wr[1] * wr[1] + wr[2] * wr[2] + wr[3] * wr[3]) * ir;
+            }
+        } else {
+            // mixed: WENO in FP32 on differences from the left cell, added back in FP64
+            const float epsf = float(kWenoEps);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                if (q == 4 && !direct) break;
+                const double c0 = s[2][q];
+                float dl, dr;
+                weno_pair<float>(float(s[0][q] - c0), float(s[1][q] - c0), 0.0f, float(s[3][q] - c0),
+                                 float(s[4][q] - c0), float(s[5][q] - c0), epsf, dl, dr);
+                wl[q] = c0 + double(dl);
+                wr[q] = c0 + double(dr);
+            }
+            if (!direct) {
+                double T[6];
+#pragma unroll
+                for (int a = 0; a < 6; ++a) T[a] = temperature(s[a], f.cT);
+                float dl, dr;
+                weno_pair<float>(float(T[0] - T[2]), float(T[1] - T[2]), 0.0f, float(T[3] - T[2]),
+                                 float(T[4] - T[2]), float(T[5] - T[2]), epsf, dl, dr);
+                const double tl = T[2] + double(dl), tr = T[2] + double(dr);
+                const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
+                wl[4] = wl[0] * tl * f.icT + 0.5 * (wl[1] * wl[1] + wl[2] * wl[2] + wl[3] * wl[3]) * il;
+                wr[4] = wr[0] * tr * f.icT + 0.5 * (wr[1] * wr[1] + wr[2] * wr[2] + wr[3] * wr[3]) * ir;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            f.rec[q][x.c] = wl[q];
+            f.rec[5 + q][x.c] = wr[q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Flux at the interface between cell c and its +1 neighbour along DIR
+// (derivsX/Y/Z, update.cpp:201-453, and flux, GKMflux.cpp:11-215).
+// Transverse lines: x sweep N,S = y+-1, F,B = z+-1; y sweep N,S = x-+1 with
+// DWy = -(N-S)/2dx, F,B = z+-1; z sweep N,S = x+-1, F,B = y+-1 (the
+// reference's assignment) or, with GKS_FIX_ZSWEEP, N,S = y+-1, F,B = x+-1.
+// Momentum is rotated into slot 1 for y (rho v) and z (rho w).
+// ---------------------------------------------------------------------------
+template <int DIR>
+__device__ __forceinline__ void transverse(const Cell &x, int flags, long long &n, long long &s,
+                                           long long &fr, long long &bk)
+{
+    if (DIR == 0) {
+        n = shift(x, 1, 0, 0); s = shift(x, -1, 0, 0);
+        fr = shift(x, 0, 0, 1); bk = shift(x, 0, 0, -1);
+    } else if (DIR == 1) {
+        n = shift(x, 0, -1, 0); s = shift(x, 0, 1, 0);
+        fr = shift(x, 0, 0, 1); bk = shift(x, 0, 0, -1);
+    } else {
+        if (flags & GKS_FIX_ZSWEEP) {
+            n = shift(x, 1, 0, 0); s = shift(x, -1, 0, 0);
+            fr = shift(x, 0, 1, 0); bk = shift(x, 0, -1, 0);
+        } else {
+            n = shift(x, 0, 1, 0); s = shift(x, 0, -1, 0);
+            fr = shift(x, 1, 0, 0); bk = shift(x, -1, 0, 0);
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void rot5(T v[5], int r)
+{
+    const T t = v[1];
+    v[1] = v[r];
+    v[r] = t;
+}
+
+template <int DIR, int PREC>
+__global__ void __launch_bounds__(128) k_flux(Batch b)
+{
+    using S = typename std::conditional<PREC == 0, double, float>::type;
+    constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
+    const double ysign = DIR == 1 ? -0.5 : 0.5;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
+        const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
+        const Cell x = decode(it - f.base, f.nc);
+        const long long c = x.c, c1 = along<DIR>(x, 1);
+        long long cn, cs, cf, cb;
+        transverse<DIR>(x, f.flags, cn, cs, cf, cb);
+        const double idx = f.inv_dx;
+
+        double WL[5], WR[5], Wl[5], Wr[5];
+        S DWl[3][5], DWr[3][5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            WL[q] = __ldg(f.W[q] + c);
+            WR[q] = __ldg(f.W[q] + c1);
+            Wl[q] = __ldg(f.rec[q] + c);
+            Wr[q] = __ldg(f.rec[5 + q] + c);
+            DWl[0][q] = S(2.0 * (Wl[q] - WL[q]) * idx);
+            DWr[0][q] = S(2.0 * (WR[q] - Wr[q]) * idx);
+            DWl[1][q] = S(ysign * (__ldg(f.rec[q] + cn) - __ldg(f.rec[q] + cs)) * idx);
+            DWr[1][q] = S(ysign * (__ldg(f.rec[5 + q] + cn) - __ldg(f.rec[5 + q] + cs)) * idx);
+            DWl[2][q] = S(0.5 * (__ldg(f.rec[q] + cf) - __ldg(f.rec[q] + cb)) * idx);
+            DWr[2][q] = S(0.5 * (__ldg(f.rec[5 + q] + cf) - __ldg(f.rec[5 + q] + cb)) * idx);
+        }
+        // collision time at the left cell, before rotation (update.cpp:262-264)
+        double tau0;
+        {
+            const double ri = __drcp_rn(WL[0]);
+            const double P = f.gm1 * (WL[4] - 0.5 * (WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]) * ri);
+            const double T = P * ri * (1.0 / f.R);
+            tau0 = viscosity(f, T) * __drcp_rn(P);
+        }
+        if (ROT) {
+            rot5(WL, ROT); rot5(WR, ROT); rot5(Wl, ROT); rot5(Wr, ROT);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { rot5(DWl[d], ROT); rot5(DWr[d], ROT); }
+        }
+        FluxConst fc;
+        fc.gm1 = f.gm1;
+        fc.dt = f.dt;
+        fc.dx = f.dx;
+        fc.kA = f.kA;
+        fc.K = f.K;
+        double F[5];
+        gks_flux<S>(WL, WR, Wl, Wr, DWl, DWr, tau0, fc, F);
+        if (ROT) rot5(F, ROT);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) f.F[DIR * 5 + q][c] = F[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Conservative update of the interior (update.cpp:455-469), evaluated in the
+// reference's order: W - (1/dx)*(Fx - Fx[i-1] + Fy - Fy[j-1] + Fz - Fz[k-1]).
+// Also flags non-finite or non-positive density / pressure.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_update(Batch b)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
+        const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
+        const Cell x = decode(it - f.base, f.nc);
+        const long long c = x.c;
+        const long long cx = shift(x, 0, -1, 0), cy = shift(x, -1, 0, 0), cz = shift(x, 0, 0, -1);
+        double w[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double d = __dsub_rn(f.F[q][c], f.F[q][cx]);
+            d = __dadd_rn(d, f.F[5 + q][c]);
+            d = __dsub_rn(d, f.F[5 + q][cy]);
+            d = __dadd_rn(d, f.F[10 + q][c]);
+            d = __dsub_rn(d, f.F[10 + q][cz]);
+            w[q] = __dsub_rn(f.W[q][c], __dmul_rn(f.inv_dx, d));
+            f.W[q][c] = w[q];
+        }
+        const double p = f.gm1 * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) / w[0]);
+        if (!(w[0] > 0.0) || !(p > 0.0) || !isfinite(w[0] + w[1] + w[2] + w[3] + w[4]))
+            atomicOr(b.err, 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion: padded staging (5 x nt^3) <-> interior.
+// ---------------------------------------------------------------------------
+__global__ void k_gather(FieldDev f, const double *__restrict__ stage)
+{
+    const int nc = f.nc, nt = nc + 6;
+    const long long Nt = (long long)nt * nt * nt;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
+        const Cell x = decode(c, nc);
+        const long long p = ((long long)(x.j + 3) * nt + (x.i + 3)) * nt + (x.k + 3);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) f.W[q][c] = stage[q * Nt + p];
+    }
+}
+
+__global__ void k_scatter(FieldDev f, double *__restrict__ stage)
+{
+    const int nc = f.nc, nt = nc + 6;
+    const long long Nt = (long long)nt * nt * nt;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < Nt; p += stride) {
+        const int kk = int(p % nt);
+        const int ii = int((p / nt) % nt);
+        const int jj = int(p / ((long long)nt * nt));
+        const long long c = ((long long)wrap(jj - 3, nc) * nc + wrap(ii - 3, nc)) * nc + wrap(kk - 3, nc);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) stage[q * Nt + p] = f.W[q][c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Largest |u| + c (timestep, update.cpp:1057-1079), each operation rounded as
+// the reference writes it so that dt matches bit for bit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void k_maxwave(FieldDev f, unsigned long long *out)
+{
+    double m = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
+        const double den = f.W[0][c];
+        const double u = __ddiv_rn(f.W[1][c], den), v = __ddiv_rn(f.W[2][c], den), w = __ddiv_rn(f.W[3][c], den);
+        const double vsq = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
+        const double P = __dmul_rn(__dmul_rn(den, f.gm1), __dsub_rn(__ddiv_rn(f.W[4][c], den), __dmul_rn(0.5, vsq)));
+        const double val = __dadd_rn(__dsqrt_rn(vsq), __dsqrt_rn(__ddiv_rn(__dmul_rn(f.gam, P), den)));
+        m = val > m ? val : m;
+    }
+    m = warp_max(m);
+    __shared__ double sm[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sm[wid] = m;
+    __syncthreads();
+    if (wid == 0) {
+        m = lane < (blockDim.x >> 5) ? sm[lane] : 0.0;
+        m = warp_max(m);
+        if (lane == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Statistics (PrintStats, update.cpp:638-784).  Velocity gradients are the
+// node slopes of the natural cubic spline through each padded grid line
+// (nt = nc + 6 points, periodic ghosts), the interpolant the reference builds
+// with einspline (Interpolation.cpp:3-31); at nodes a tensor-product natural
+// spline reduces to these 1-D slopes.  Scratch layout: [0..2] u, v, w;
+// [3 + 3*comp + axis] d(comp)/d(axis), axis 0 = y, 1 = x, 2 = z.
+// ---------------------------------------------------------------------------
+__global__ void k_velocity(FieldDev f, double *scr)
+{
+    const long long n = f.ncell;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
+        const double d = f.W[0][c];
+        scr[c] = f.W[1][c] / d;
+        scr[n + c] = f.W[2][c] / d;
+        scr[2 * n + c] = f.W[3][c] / d;
+    }
+}
+
+// One thread per grid line along `axis`, solving the three velocity
+// components' slope systems with the Thomas algorithm (pivots precomputed):
+//   2 m0 + m1 = s (f1 - f0);  m_{p-1} + 4 m_p + m_{p+1} = s (f_{p+1} - f_{p-1});
+//   m_{n-2} + 2 m_{n-1} = s (f_{n-1} - f_{n-2}),  s = 3/h.
+// Forward values of interior nodes are parked in the output array and turned
+// into slopes by the backward pass.
+__global__ void k_spline(FieldDev f, double *scr, int axis)
+{
+    const int nc = f.nc, nt = nc + 6;
+    const long long n = f.ncell;
+    const long long lines = (long long)nc * nc;
+    const long long line = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= lines) return;
+    const int a = int(line / nc), bb = int(line % nc);
+    long long base, st;
+    if (axis == 0) { base = (long long)a * nc + bb; st = (long long)nc * nc; }        // along j, (i,k) = (a,b)
+    else if (axis == 1) { base = (long long)a * nc * nc + bb; st = nc; }              // along i, (j,k)
+    else { base = ((long long)a * nc + bb) * nc; st = 1; }                           // along k, (j,i)
+    const double s = f.spl_s;
+    const double *cp = f.spl_cp, *inv = f.spl_inv;
+#pragma unroll 1
+    for (int comp = 0; comp < 3; ++comp) {
+        const double *u = scr + comp * n;
+        double *g = scr + (3 + 3 * comp + axis) * n;
+        auto val = [&](int p) { return u[base + (long long)wrap(p - 3, nc) * st]; };
+        double fm = val(0), f0 = fm, fp = val(1);
+        double dp = (s * (fp - f0)) * inv[0];
+        double dlast[3];
+        for (int p = 1; p < nt; ++p) {
+            fm = f0;
+            f0 = fp;
+            double r;
+            if (p < nt - 1) {
+                fp = val(p + 1);
+                r = s * (fp - fm);
+            } else {
+                r = s * (f0 - fm);
+            }
+            dp = (r - dp) * inv[p];
+            if (p >= 3 && p <= nt - 4) g[base + (long long)(p - 3) * st] = dp;
+            else if (p >= nt - 3) dlast[p - (nt - 3)] = dp;
+        }
+        double m = dlast[2];
+        m = dlast[1] - cp[nt - 2] * m;
+        m = dlast[0] - cp[nt - 3] * m;
+        for (int p = nt - 4; p >= 3; --p) {
+            const long long o = base + (long long)(p - 3) * st;
+            m = g[o] - cp[p] * m;
+            g[o] = m;
+        }
+    }
+}
+
+constexpr int NSUM1 = 18, NSUM2 = 3;
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int N>
+__device__ __forceinline__ void block_sums(double (&v)[N], double *out)
+{
+    __shared__ double sm[N][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const double x = warp_sum(v[i]);
+        if (lane == 0) sm[i][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < N) {
+        double t = 0.0;
+        for (int w = 0; w < nw; ++w) t += sm[threadIdx.x][w];
+        out[threadIdx.x] = t;
+    }
+}
+
+__device__ __forceinline__ void cell_prim(const FieldDev &f, long long c, double &den, double &u, double &v,
+                                          double &w, double &P, double &T)
+{
+    den = f.W[0][c];
+    u = f.W[1][c] / den;
+    v = f.W[2][c] / den;
+    w = f.W[3][c] / den;
+    const double vsq = u * u + v * v + w * w;
+    P = (den * f.gm1) * (f.W[4][c] / den - 0.5 * vsq);
+    T = P / (f.R * den);
+}
+
+__global__ void k_sums1(FieldDev f, const double *scr, double *partial)
+{
+    const long long n = f.ncell;
+    double acc[NSUM1];
+#pragma unroll
+    for (int i = 0; i < NSUM1; ++i) acc[i] = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
+        double den, u, v, w, P, T;
+        cell_prim(f, c, den, u, v, w, P, T);
+        const double *g = scr + 3 * n;
+        const double dudy = g[c], dudx = g[n + c], dudz = g[2 * n + c];
+        const double dvdy = g[3 * n + c], dvdx = g[4 * n + c], dvdz = g[5 * n + c];
+        const double dwdy = g[6 * n + c], dwdx = g[7 * n + c], dwdz = g[8 * n + c];
+        const double mu = viscosity(f, T);
+        acc[0] += den * (u * u + v * v + w * w);
+        acc[1] += mu * (dudx * dudx + dudy * dudy + dudz * dudz + dvdx * dvdx + dvdy * dvdy + dvdz * dvdz +
+                        dwdx * dwdx + dwdy * dwdy + dwdz * dwdz);
+        acc[2] += dudx * dudx + 0.5 * (dudy + dvdx) * (dudy + dvdx) + 0.5 * (dudz + dwdx) * (dudz + dwdx) +
+                  0.5 * (dwdy + dvdz) * (dwdy + dvdz) + dvdy * dvdy + dwdz * dwdz;
+        const double a2 = dudx * dudx, b2 = dvdy * dvdy, c2 = dwdz * dwdz;
+        acc[3] += a2; acc[4] += a2 * dudx; acc[5] += a2 * a2;
+        acc[6] += b2; acc[7] += b2 * dvdy; acc[8] += b2 * b2;
+        acc[9] += c2; acc[10] += c2 * dwdz; acc[11] += c2 * c2;
+        acc[12] += P;
+        acc[13] += T;
+        acc[14] += 1.0 / den;
+        acc[15] += u * u + v * v + w * w;
+        acc[16] += sqrt(f.gam * P / den);
+        acc[17] += den;
+    }
+    block_sums<NSUM1>(acc, partial + (long long)blockIdx.x * NSUM1);
+}
+
+__global__ void k_sums2(FieldDev f, const double *means, double *partial)
+{
+    const long long n = f.ncell;
+    const double Pm = means[12], Tm = means[13], Vm = means[14];
+    double acc[NSUM2] = {0.0, 0.0, 0.0};
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
+        double den, u, v, w, P, T;
+        cell_prim(f, c, den, u, v, w, P, T);
+        acc[0] += (Pm - P) * (Pm - P);
+        acc[1] += (Tm - T) * (Tm - T);
+        acc[2] += (Vm - 1.0 / den) * (Vm - 1.0 / den);
+    }
+    block_sums<NSUM2>(acc, partial + (long long)blockIdx.x * NSUM2);
+}
+
+// Sum the per-block partials in a fixed order; optionally divide by ncell.
+__global__ void k_finalize(const double *partial, int nblocks, int nsum, double scale, double *out)
+{
+    const int i = threadIdx.x;
+    if (i >= nsum) return;
+    double t = 0.0;
+    for (int bidx = 0; bidx < nblocks; ++bidx) t += partial[(long long)bidx * nsum + i];
+    out[i] = t * scale;
+}
+
+__global__ void k_check(FieldDev f, int *err)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
+        double w[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) w[q] = f.W[q][c];
+        const double p = f.gm1 * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) / w[0]);
+        if (!(w[0] > 0.0) || !(p > 0.0) || !isfinite(w[0] + w[1] + w[2] + w[3] + w[4])) atomicOr(err, 2);
+    }
+}
+
+int grid_for(long long items, int block)
+{
+    long long g = (items + block - 1) / block;
+    if (g > 148LL * 32) g = 148LL * 32;
+    if (g < 1) g = 1;
+    return int(g);
+}
+
+template <int PREC>
+cudaError_t recon_dispatch(const Batch &b, int dir, LaunchCfg cfg, cudaStream_t st)
+{
+    if (dir == 0) k_recon<0, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
+    else if (dir == 1) k_recon<1, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
+    else k_recon<2, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
+    return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t flux_dispatch(const Batch &b, int dir, LaunchCfg cfg, cudaStream_t st)
+{
+    if (dir == 0) k_flux<0, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
+    else if (dir == 1) k_flux<1, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
+    else k_flux<2, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
+    return cudaGetLastError();
+}
+
+template <typename KernelT>
+cudaError_t occ(KernelT k, int block, int *n)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k, block, 0);
+}
+
+} // namespace
+
+cudaError_t launch_recon(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st)
+{
+    return prec == 0 ? recon_dispatch<0>(b, dir, cfg, st) : recon_dispatch<1>(b, dir, cfg, st);
+}
+
+cudaError_t launch_flux(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st)
+{
+    return prec == 0 ? flux_dispatch<0>(b, dir, cfg, st) : flux_dispatch<1>(b, dir, cfg, st);
+}
+
+cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st)
+{
+    k_update<<<cfg.grid, cfg.block, 0, st>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t max_resident_blocks(int kind, int dir, int prec, int block, int *n)
+{
+    if (kind == K_UPDATE) return occ(k_update, block, n);
+    if (kind == K_RECON) {
+        if (prec == 0) return dir == 0 ? occ(k_recon<0, 0>, block, n) : dir == 1 ? occ(k_recon<1, 0>, block, n) : occ(k_recon<2, 0>, block, n);
+        return dir == 0 ? occ(k_recon<0, 1>, block, n) : dir == 1 ? occ(k_recon<1, 1>, block, n) : occ(k_recon<2, 1>, block, n);
+    }
+    if (prec == 0) return dir == 0 ? occ(k_flux<0, 0>, block, n) : dir == 1 ? occ(k_flux<1, 0>, block, n) : occ(k_flux<2, 0>, block, n);
+    return dir == 0 ? occ(k_flux<0, 1>, block, n) : dir == 1 ? occ(k_flux<1, 1>, block, n) : occ(k_flux<2, 1>, block, n);
+}
+
+cudaError_t launch_gather(const FieldDev &f, const double *stage, cudaStream_t st)
+{
+    k_gather<<<grid_for(f.ncell, 256), 256, 0, st>>>(f, stage);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const FieldDev &f, double *stage, cudaStream_t st)
+{
+    const long long nt = f.nc + 6;
+    k_scatter<<<grid_for(nt * nt * nt, 256), 256, 0, st>>>(f, stage);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, cudaStream_t st)
+{
+    k_maxwave<<<grid_for(f.ncell, 256), 256, 0, st>>>(f, out_bits);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, cudaStream_t st)
+{
+    const int block = 256;
+    const int grid = grid_for(f.ncell, block);
+    k_velocity<<<grid, block, 0, st>>>(f, scratch);
+    const long long lines = (long long)f.nc * f.nc;
+    const int lgrid = int((lines + 127) / 128);
+    for (int axis = 0; axis < 3; ++axis) k_spline<<<lgrid, 128, 0, st>>>(f, scratch, axis);
+    k_sums1<<<grid, block, 0, st>>>(f, scratch, partial);
+    k_finalize<<<1, 32, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
+    double *partial2 = partial + (long long)grid * NSUM1;
+    k_sums2<<<grid, block, 0, st>>>(f, sums, partial2);
+    k_finalize<<<1, 32, 0, st>>>(partial2, grid, NSUM2, 1.0, sums + NSUM1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check(const FieldDev &f, int *err, cudaStream_t st)
+{
+    k_check<<<grid_for(f.ncell, 256), 256, 0, st>>>(f, err);
+    return cudaGetLastError();
+}
+
+} // namespace gks

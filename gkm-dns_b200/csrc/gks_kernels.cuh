@@ -1,0 +1,74 @@
+// Field descriptors and kernel launchers shared by the kernels (gks_kernels.cu)
+// and the C ABI (gks_capi.cu).
+//
+// Device layout of a field: five arrays of nc^3 doubles (interior cells only,
+// index (j*nc + i)*nc + k, j = y, i = x, k = z), the periodic halo being
+// applied by index wrapping inside the kernels.  Per field the context also
+// holds a reconstruction buffer (10 arrays: the left and right WENO states of
+// the interface at the high side of every cell, for the sweep in progress)
+// and a flux buffer (15 arrays: the x, y and z interface fluxes of the step).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gks {
+
+struct FieldDev {
+    double *W[5];     // state, interior layout
+    double *rec[10];  // Wl[0..4], Wr[0..4] of the current sweep
+    double *F[15];    // Fx[0..4], Fy[0..4], Fz[0..4]
+    const double *spl_cp;   // natural-spline Thomas coefficients, nt entries
+    const double *spl_inv;  // reciprocal pivots, nt entries
+    long long base;   // first work item (cell) of this field in the batch
+    long long ncell;  // nc^3
+    int nc;
+    int K;
+    int visc_law;     // 0 Sutherland, 1 power law
+    int flags;        // GKS_FIX_ZSWEEP | GKS_DIRECT_ENERGY
+    double dx, inv_dx, dt;
+    double gam, gm1, R, cT, icT; // cT = (gam-1)/R, icT = R/(gam-1)
+    double T0, iT0, mu0, visc_exp;
+    double kA;        // pr_factor * 4/(K+3)
+    double spl_s;     // 3/h of the spline grid
+};
+
+struct Batch {
+    FieldDev *fields; // device array
+    int nfields;
+    long long total;  // sum of ncell
+    int *err;         // device error word (bit 0: non-finite / non-positive state after update)
+};
+
+// Launch configuration chosen by the tuner per kernel kind.
+struct LaunchCfg {
+    int block;
+    int grid;
+};
+
+enum KernelKind { K_RECON = 0, K_FLUX = 1, K_UPDATE = 2, K_KINDS = 3 };
+
+// Stage launchers (asynchronous on `st`).  prec: 0 FP64, 1 mixed.
+cudaError_t launch_recon(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);
+cudaError_t launch_flux(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);
+cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st);
+
+// Occupancy-based persistent grid for a kernel kind.
+cudaError_t max_resident_blocks(int kind, int dir, int prec, int block, int *blocks_per_sm);
+
+// Layout conversion of one field: padded host layout (5 x nt^3, contiguous) <-> interior.
+cudaError_t launch_gather(const FieldDev &f, const double *stage, cudaStream_t st);
+cudaError_t launch_scatter(const FieldDev &f, double *stage, cudaStream_t st);
+
+// max(|u| + c) over the interior of one field into *out_bits (uint64 image of a positive double;
+// *out_bits must be zero on entry).
+cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, cudaStream_t st);
+
+// Statistics of one field.  scratch: 12 * nc^3 doubles; partial: >= 2 * 32 * nblocks doubles.
+// Writes 16 sums of the first pass and 3 of the second into sums[0..18].
+cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, cudaStream_t st);
+
+// Scan a field for non-finite values or non-positive density / pressure; sets bit 1 of *err.
+cudaError_t launch_check(const FieldDev &f, int *err, cudaStream_t st);
+
+} // namespace gks

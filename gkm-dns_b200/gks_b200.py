@@ -1,0 +1,218 @@
+"""Python binding of the gks_b200 C ABI (include/gks_b200.h) through ctypes.
+
+The binding mirrors the reference's run loop objects: a ``Solver`` owns one
+device context (one field, or an ensemble of fields of different sizes) and
+exposes the calls the reference's driver makes each step -- upload of the
+conservative fields in the reference's padded layout, the time step from the
+CFL condition, the step itself, download, and the diagnostics PrintStats
+prints.  There is no fallback: if ``lib/libgks_b200.so`` is missing or no GPU
+is present, construction raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgks_b200.so")
+
+FP64 = 0
+MIXED = 1
+FIX_ZSWEEP = 1
+DIRECT_ENERGY = 2
+VISC_SUTHERLAND = 0
+VISC_POWER = 1
+PR_FACTOR_CPU = 1.0 / 0.7  # GKMflux.cpp:289
+PR_FACTOR_GPU = 1.0        # GPUupdate.cu:839
+
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ESTATE", -5: "ENONFINITE", -6: "ETOOBIG"}
+
+STATS_FIELDS = ["tke", "diss", "skew_u", "skew_v", "skew_w", "kurt_u", "kurt_v", "kurt_w",
+                "prms", "trms", "vrms", "sijsij", "mach_t", "rho_mean"]
+
+
+class GksError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gks error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Phys(ctypes.Structure):
+    _fields_ = [
+        ("nc", ctypes.c_int), ("K", ctypes.c_int), ("visc_law", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("gam", ctypes.c_double), ("R", ctypes.c_double), ("T0", ctypes.c_double), ("mu0", ctypes.c_double),
+        ("visc_exp", ctypes.c_double), ("pr_factor", ctypes.c_double),
+        ("p0", ctypes.c_double), ("den0", ctypes.c_double), ("Mt", ctypes.c_double), ("t0", ctypes.c_double),
+    ]
+
+
+class StatsOut(ctypes.Structure):
+    _fields_ = [
+        ("tke", ctypes.c_double), ("diss", ctypes.c_double), ("skew", ctypes.c_double * 3),
+        ("kurt", ctypes.c_double * 3), ("prms", ctypes.c_double), ("trms", ctypes.c_double),
+        ("vrms", ctypes.c_double), ("sijsij", ctypes.c_double), ("mach_t", ctypes.c_double),
+        ("rho_mean", ctypes.c_double),
+    ]
+
+    def as_array(self) -> np.ndarray:
+        return np.array([self.tke, self.diss, *self.skew, *self.kurt, self.prms, self.trms, self.vrms,
+                         self.sijsij, self.mach_t, self.rho_mean])
+
+
+DP = ctypes.POINTER(ctypes.c_double)
+DP5 = DP * 5
+
+# every symbol the header declares, with (restype, argtypes)
+SIGNATURES = {
+    "gks_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(Phys),
+                                  ctypes.c_int, ctypes.c_int]),
+    "gks_destroy": (None, [ctypes.c_void_p]),
+    "gks_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gks_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
+    "gks_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
+    "gks_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, DP]),
+    "gks_set_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]),
+    "gks_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "gks_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StatsOut)]),
+    "gks_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "gks_check": (ctypes.c_int, [ctypes.c_void_p]),
+    "gks_device_fields": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
+    "gks_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "gks_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with __graft_entry__.build() (make -C gkm-dns_b200)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def phys_from_case(case, visc_law=VISC_SUTHERLAND, visc_exp=0.76, pr_factor=PR_FACTOR_CPU) -> Phys:
+    """gks_phys from a gks_ic.DhitCase (or any object with its attributes)."""
+    return Phys(nc=case.nc, K=case.K, visc_law=visc_law, reserved=0, gam=case.gam, R=287.0, T0=case.T0,
+                mu0=case.mu0, visc_exp=visc_exp, pr_factor=pr_factor, p0=case.p0, den0=case.rho0, Mt=case.Mt,
+                t0=case.t0)
+
+
+def _ptrs(W: np.ndarray) -> DP5:
+    assert W.dtype == np.float64 and W.flags["C_CONTIGUOUS"] and W.shape[0] == 5
+    return DP5(*[W[q].ctypes.data_as(DP) for q in range(5)])
+
+
+@dataclasses.dataclass
+class _Field:
+    nc: int
+
+
+class Solver:
+    """One context on the current CUDA device holding one or more fields."""
+
+    def __init__(self, phys, precision: int = FP64, flags: int = 0):
+        lib = load_library()
+        if isinstance(phys, Phys):
+            phys = [phys]
+        arr = (Phys * len(phys))(*phys)
+        h = ctypes.c_void_p()
+        rc = lib.gks_create(ctypes.byref(h), len(phys), arr, precision, flags)
+        if rc != 0:
+            raise GksError(rc, "gks_create failed (no CUDA device, bad constants or out of memory)")
+        self._lib = lib
+        self._h = h
+        self.fields = [_Field(p.nc) for p in phys]
+        self.precision = precision
+        self.flags = flags
+
+    def _ck(self, rc):
+        if rc != 0:
+            msg = self._lib.gks_last_error(self._h)
+            raise GksError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if self._h:
+            self._lib.gks_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # state ---------------------------------------------------------------
+    def upload(self, W: np.ndarray, f: int = 0):
+        """W: (5, nt, nt, nt) float64 in the reference's padded layout."""
+        nt = self.fields[f].nc + 6
+        if W.shape != (5, nt, nt, nt):
+            raise ValueError(f"expected shape {(5, nt, nt, nt)}, got {W.shape}")
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        self._ck(self._lib.gks_upload(self._h, f, _ptrs(W)))
+
+    def download(self, f: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        nt = self.fields[f].nc + 6
+        if out is None:
+            out = np.empty((5, nt, nt, nt))
+        self._ck(self._lib.gks_download(self._h, f, _ptrs(out)))
+        return out
+
+    def timestep(self, cfl: float, f: int = 0) -> float:
+        dt = ctypes.c_double()
+        self._ck(self._lib.gks_timestep(self._h, f, cfl, ctypes.byref(dt)))
+        return dt.value
+
+    def set_dt(self, dt: float, f: int = 0):
+        self._ck(self._lib.gks_set_dt(self._h, f, dt))
+
+    def step(self, nsteps: int = 1):
+        self._ck(self._lib.gks_step(self._h, nsteps))
+
+    def sync(self):
+        self._ck(self._lib.gks_sync(self._h))
+
+    def check(self):
+        self._ck(self._lib.gks_check(self._h))
+
+    def stats(self, f: int = 0) -> dict:
+        out = StatsOut()
+        self._ck(self._lib.gks_stats(self._h, f, ctypes.byref(out)))
+        return dict(zip(STATS_FIELDS, out.as_array()))
+
+    def stats_array(self, f: int = 0) -> np.ndarray:
+        out = StatsOut()
+        self._ck(self._lib.gks_stats(self._h, f, ctypes.byref(out)))
+        return out.as_array()
+
+    def device_fields(self, f: int = 0):
+        arr = DP5()
+        self._ck(self._lib.gks_device_fields(self._h, f, arr))
+        return [ctypes.cast(arr[q], ctypes.c_void_p).value for q in range(5)]
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._ck(self._lib.gks_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def set_stream(self, stream: int | None):
+        self._ck(self._lib.gks_set_stream(self._h, ctypes.c_void_p(stream or 0)))

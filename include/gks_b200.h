@@ -1,0 +1,144 @@
+/*
+ * gks_b200: B200 (sm_100a) implementation of the GKM-DNS per-step hot path --
+ * WENO-SYMOO interface reconstruction in the x/y/z sweeps, the BGK gas-kinetic
+ * interface flux and the conservative update -- behind a plain C ABI.
+ *
+ * Replaces, in the reference (nishantp9/GKM-DNS, WENO tree):
+ *   void evolve(ptype *W[5], DevAlloc *dev, ptype dt)        weno/src/GPUupdate.h:33
+ *   void evolveEulerian(ptype *W[5], ptype *Fx[5], ...)       weno/src/update.h:16 (CPU path)
+ *   class DevAlloc (50 device buffers)                        weno/src/GPUAlloc.h:6-22
+ *   void timestep(ptype *W[5])                                weno/src/update.cpp:1057-1079
+ *   void PrintStats(ptype *W[5], UBspline_3d_d *splinep[5])   weno/src/update.cpp:638-784
+ *   void HaloTransfer(...) on one periodic rank               weno/src/update.cpp:894-1054
+ * The compatibility shim with the reference's own evolve()/DevAlloc
+ * signatures is gkm-dns_b200/driver/gks_compat.h.
+ *
+ * Conventions
+ * - A field is the reference's padded block: nt = nc + 6 cells per edge
+ *   (3 ghost layers), linear index (j*nt + i)*nt + k with j = y slowest,
+ *   i = x, k = z fastest (weno/src/param.h:37), five separate double arrays
+ *   rho, rho u, rho v, rho w, rho E.  The domain is the periodic cube
+ *   [0, 2 pi)^3, dx = 2 pi / nc.
+ * - The state stays resident on the device between calls; upload/download
+ *   convert between the host's padded layout and the device layout
+ *   (interior only; the periodic halo is applied inside the kernels).
+ * - One context holds one field or a batch of independent fields of
+ *   different sizes (an ensemble); every stage of a step advances all fields
+ *   of the context in one launch.
+ * - Every call returns 0 on success or a negative GKS_E* code; the message of
+ *   the last failure is gks_last_error(ctx).  A context is not thread-safe.
+ */
+#ifndef GKS_B200_H
+#define GKS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GKS_ABI_VERSION 1
+
+/* precision */
+#define GKS_FP64 0  /* every operation in FP64 (parity path) */
+#define GKS_MIXED 1 /* WENO weights, slope solves, slope moments in FP32; moments, erfc, update, reductions FP64 */
+
+/* flags: the reference's behaviour is the default (0) */
+#define GKS_FIX_ZSWEEP 1    /* z sweep: transverse slopes along the rotated frame's axes
+                               (the reference uses d/dx and d/dy in swapped slots, update.cpp:380-421) */
+#define GKS_DIRECT_ENERGY 2 /* WENO on rho E directly, as the reference GPU kernel does
+                               (GPUupdate.cu:542-546); default is WENO of T (update.cpp:560-619) */
+
+/* viscosity law */
+#define GKS_VISC_SUTHERLAND 0 /* mu0 (T/T0)^1.5 (T0+110.4)/(T+110.4), update.cpp:263 */
+#define GKS_VISC_POWER 1      /* mu0 (T/T0)^visc_exp, GKM/CUDA GKM/src/CPUupdate.cpp:65 */
+
+/* error codes */
+#define GKS_OK 0
+#define GKS_EINVAL (-1)   /* bad argument */
+#define GKS_ECUDA (-2)    /* CUDA runtime failure */
+#define GKS_ENOMEM (-3)   /* device allocation failed */
+#define GKS_ESTATE (-4)   /* call out of order (e.g. step before upload / dt) */
+#define GKS_ENONFINITE (-5) /* non-finite or non-positive density/pressure found */
+#define GKS_ETOOBIG (-6)  /* size beyond a fixed capacity */
+
+typedef struct gks_ctx gks_ctx;
+
+/* Physical constants of one field; the reference reads them from
+ * InitialConditions/params and param.h (FlowField.cpp:15-50). */
+typedef struct {
+    int nc;           /* interior cells per edge (>= 4) */
+    int K;            /* internal degrees of freedom, int((5-3 gam)/(gam-1)) (FlowField.cpp:41) */
+    int visc_law;     /* GKS_VISC_* */
+    int reserved;
+    double gam;       /* ratio of specific heats */
+    double R;         /* gas constant (287, param.h:18) */
+    double T0;        /* p0 / (R rho0) (FlowField.cpp:46) */
+    double mu0;       /* viscosity at T0 */
+    double visc_exp;  /* exponent of GKS_VISC_POWER */
+    double pr_factor; /* factor on the energy slope coefficient: 1/0.7 as the CPU reference
+                         (GKMflux.cpp:289), 1.0 as the GPU reference (GPUupdate.cu:839) */
+    double p0, den0, Mt, t0; /* normalisation of the statistics (update.cpp:772-776) */
+} gks_phys;
+
+/* Diagnostics of one field (PrintStats, update.cpp:638-784). */
+typedef struct {
+    double tke;      /* <rho |u|^2> */
+    double diss;     /* <mu du_i/dx_j du_i/dx_j> */
+    double skew[3];  /* <(du/dx)^3>/<(du/dx)^2>^1.5, same for dv/dy, dw/dz */
+    double kurt[3];  /* <(du/dx)^4>/<(du/dx)^2>^2, ... */
+    double prms;     /* rms pressure / (gam p0 Mt^2) */
+    double trms;     /* rms temperature / ((gam-1) T0 Mt^2) */
+    double vrms;     /* rms specific volume / (Mt^2 / den0) */
+    double sijsij;   /* <S_ij S_ij> (computed, not printed, by the reference) */
+    double mach_t;   /* sqrt(<|u|^2>) / <c> (not in the reference's printout) */
+    double rho_mean; /* <rho> */
+} gks_stats_out;
+
+/* Create a context for nfields fields with the given constants (one gks_phys
+ * per field).  precision is GKS_FP64 or GKS_MIXED; flags a GKS_FIX_* mask. */
+int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, int flags);
+void gks_destroy(gks_ctx *ctx);
+const char *gks_last_error(const gks_ctx *ctx);
+
+/* Host <-> device state of field f, reference padded layout (ghosts are
+ * ignored on upload and written as the periodic image on download, i.e. the
+ * state after the reference's HaloTransfer). */
+int gks_upload(gks_ctx *ctx, int f, double *const W[5]);
+int gks_download(gks_ctx *ctx, int f, double *const W[5]);
+
+/* Time step: dt = cfl*dx/max(|u|+c) over the interior (timestep,
+ * update.cpp:1057-1079); the result is also made the step's dt. */
+int gks_timestep(gks_ctx *ctx, int f, double cfl, double *dt_out);
+int gks_set_dt(gks_ctx *ctx, int f, double dt);
+
+/* Advance every field of the context by nsteps single-stage steps
+ * (evolveEulerian, update.cpp:194-199): three fused reconstruction + flux
+ * sweeps and the conservative update per step, captured once as a CUDA
+ * graph.  Asynchronous on the context's stream. */
+int gks_step(gks_ctx *ctx, int nsteps);
+
+/* Diagnostics of field f on the current state (synchronises). */
+int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out);
+
+/* Wait for all work of the context. */
+int gks_sync(gks_ctx *ctx);
+
+/* Check every field for non-finite or non-positive density / pressure; returns
+ * GKS_ENONFINITE and names the first offending field in gks_last_error. */
+int gks_check(gks_ctx *ctx);
+
+/* Device-resident interior arrays of field f (nc^3 doubles each, index
+ * (j*nc + i)*nc + k), for callers that keep the state on the GPU. */
+int gks_device_fields(gks_ctx *ctx, int f, double *dW[5]);
+
+/* Run subsequent work on a caller-provided cudaStream_t (NULL: the context's
+ * own stream).  Invalidates the captured step graph. */
+int gks_set_stream(gks_ctx *ctx, void *stream);
+
+/* The cudaStream_t the context launches on (for event timing by callers). */
+int gks_get_stream(gks_ctx *ctx, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,190 @@
+"""Python access to the CPU oracle (test infrastructure only).
+
+Two checkers live under oracle/:
+
+* ``build/liboracle.so``: the plain-C restatement of the reference hot path
+  (gks_oracle.c), loaded through ctypes;
+* ``_ref/ref_harness``: the reference's own CPU path compiled from its sources
+  (see the Makefile), driven as a subprocess.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this
+module, and only to check or time against; the product never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
+REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+REF_HARNESS_FAST = os.path.join(HERE, "_ref", "ref_harness_fast")
+
+VISC_SUTHERLAND = 0
+VISC_POWER = 1
+FIX_ZSWEEP = 1
+DIRECT_ENERGY = 2
+PR_FACTOR_CPU = 1.0 / 0.7  # GKMflux.cpp:289
+PR_FACTOR_GPU = 1.0        # GPUupdate.cu:839
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [
+        ("nc", ctypes.c_int), ("K", ctypes.c_int), ("visc_law", ctypes.c_int), ("flags", ctypes.c_int),
+        ("gam", ctypes.c_double), ("R", ctypes.c_double), ("dx", ctypes.c_double),
+        ("T0", ctypes.c_double), ("mu0", ctypes.c_double), ("visc_exp", ctypes.c_double),
+        ("pr_factor", ctypes.c_double), ("p0", ctypes.c_double), ("den0", ctypes.c_double),
+        ("Mt", ctypes.c_double), ("t0", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.orc_weno.argtypes = [dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp]
+        L.orc_flux.argtypes = [dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
+        L.orc_halo.argtypes = [dp, ctypes.c_int]
+        L.orc_step.argtypes = [dp, ctypes.POINTER(OrcParams), ctypes.c_double, dp]
+        L.orc_maxval.argtypes = [dp, ctypes.POINTER(OrcParams)]
+        L.orc_maxval.restype = ctypes.c_double
+        L.orc_stats.argtypes = [dp, ctypes.POINTER(OrcParams), dp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def params(nc, gam, mu0, p0, den0=1.0, Mt=0.3, t0=1.0, visc_law=VISC_SUTHERLAND, visc_exp=0.76,
+           pr_factor=PR_FACTOR_CPU, flags=0, R=287.0) -> OrcParams:
+    dx = 2.0 * (np.arctan(1.0) * 4.0) / nc
+    K = int((5.0 - 3.0 * gam) / (gam - 1.0))
+    T0 = p0 / (R * den0)
+    return OrcParams(nc, K, visc_law, flags, gam, R, dx, T0, mu0, visc_exp, pr_factor, p0, den0, Mt, t0)
+
+
+def weno(stencils: np.ndarray, gam=1.4, R=287.0, direct_energy=False):
+    """stencils (n, 6, 5) -> (wl, wr) each (n, 5)."""
+    s = np.ascontiguousarray(stencils, dtype=np.float64)
+    n = s.shape[0]
+    wl = np.empty((n, 5))
+    wr = np.empty((n, 5))
+    L = lib()
+    for c in range(n):
+        L.orc_weno(_p(s[c]), gam, R, int(direct_energy), _p(wl[c]), _p(wr[c]))
+    return wl, wr
+
+
+def flux(inputs: np.ndarray, gam=1.4, K=2, pr_factor=PR_FACTOR_CPU):
+    """inputs (n, 53) -> F (n, 5)."""
+    x = np.ascontiguousarray(inputs, dtype=np.float64)
+    F = np.empty((x.shape[0], 5))
+    L = lib()
+    for c in range(x.shape[0]):
+        L.orc_flux(_p(x[c]), gam, K, pr_factor, _p(F[c]))
+    return F
+
+
+def step(W: np.ndarray, prm: OrcParams, dt: float, nsteps: int = 1) -> np.ndarray:
+    """Advance a padded (5, nt, nt, nt) block in place by nsteps steps."""
+    assert W.shape[0] == 5 and W.flags["C_CONTIGUOUS"]
+    scratch = np.zeros((15,) + W.shape[1:])
+    L = lib()
+    for _ in range(nsteps):
+        L.orc_step(_p(W), ctypes.byref(prm), dt, _p(scratch))
+    return W
+
+
+def maxval(W: np.ndarray, prm: OrcParams) -> float:
+    return lib().orc_maxval(_p(np.ascontiguousarray(W)), ctypes.byref(prm))
+
+
+def stats(W: np.ndarray, prm: OrcParams) -> np.ndarray:
+    out = np.empty(14)
+    lib().orc_stats(_p(np.ascontiguousarray(W)), ctypes.byref(prm), _p(out))
+    return out
+
+
+def halo(W: np.ndarray, nc: int) -> np.ndarray:
+    lib().orc_halo(_p(W), nc)
+    return W
+
+
+# --- the reference build ---------------------------------------------------
+
+def have_ref() -> bool:
+    return os.path.exists(REF_HARNESS)
+
+
+def ref_run(casedir: str, nsteps: int, cfl: float, dumps, stats_on=True, outdir=None):
+    """Run the reference binary; returns dict(meta, stats, dumps, stdout)."""
+    outdir = outdir or tempfile.mkdtemp(prefix="gksref_")
+    os.makedirs(outdir, exist_ok=True)
+    dl = ",".join(str(d) for d in dumps) if dumps else ","
+    cp = subprocess.run([REF_HARNESS, "run", os.path.abspath(casedir), os.path.abspath(outdir), str(nsteps),
+                         repr(cfl), "1" if stats_on else "0", dl],
+                        check=True, capture_output=True, text=True)
+    meta = {}
+    with open(os.path.join(outdir, "meta.txt")) as f:
+        for line in f:
+            k, v = line.split()
+            meta[k] = float(v)
+    st = np.fromfile(os.path.join(outdir, "stats.bin"), dtype=np.float64).reshape(-1, 9)
+    nc = int(meta["nc"])
+    nt = nc + 6
+    out = {}
+    for d in dumps:
+        out[d] = np.fromfile(os.path.join(outdir, f"W_{d}.bin"), dtype=np.float64).reshape(5, nt, nt, nt)
+    lines = [ln for ln in cp.stdout.splitlines() if ln.strip() and ln.strip()[0].isdigit()]
+    return {"meta": meta, "stats": st, "dumps": out, "stdout": lines, "outdir": outdir}
+
+
+def _blob(path, n, header: bytes, rows: np.ndarray):
+    with open(path, "wb") as f:
+        f.write(struct.pack("<i", n))
+        f.write(header)
+        f.write(np.ascontiguousarray(rows, dtype="<f8").tobytes())
+
+
+def ref_weno(stencils: np.ndarray, gam=1.4):
+    n = stencils.shape[0]
+    d = tempfile.mkdtemp(prefix="gksweno_")
+    _blob(os.path.join(d, "in"), n, struct.pack("<d", gam), stencils.reshape(n, 30))
+    subprocess.run([REF_HARNESS, "weno", os.path.join(d, "in"), os.path.join(d, "out")], check=True)
+    o = np.fromfile(os.path.join(d, "out"), dtype=np.float64).reshape(n, 10)
+    return o[:, :5], o[:, 5:]
+
+
+def ref_flux(inputs: np.ndarray, gam=1.4, K=2):
+    n = inputs.shape[0]
+    d = tempfile.mkdtemp(prefix="gksflux_")
+    _blob(os.path.join(d, "in"), n, struct.pack("<dd", gam, float(K)), inputs.reshape(n, 53))
+    subprocess.run([REF_HARNESS, "flux", os.path.join(d, "in"), os.path.join(d, "out")], check=True)
+    return np.fromfile(os.path.join(d, "out"), dtype=np.float64).reshape(n, 5)
+
+
+def ref_time(casedir: str, nsteps: int, slabs: int, cfl: float, fast=True) -> dict:
+    import json
+    exe = REF_HARNESS_FAST if fast else REF_HARNESS
+    cp = subprocess.run([exe, "time", os.path.abspath(casedir), str(nsteps), str(slabs), repr(cfl)],
+                        check=True, capture_output=True, text=True)
+    return json.loads(cp.stdout.strip().splitlines()[-1])

@@ -1,0 +1,261 @@
+"""GPU parity of the step, time step and diagnostics against the oracle.
+
+Every call goes through the C ABI (include/gks_b200.h) via gks_b200.  The
+reference (pinned bit for bit to the oracle, test_oracle_pin.py) defines the
+answers: golden fixtures where they exist, the oracle run on the same input
+otherwise.
+
+Tolerances: the FP64 path must reproduce the reference to 1e-12 relative to
+each conserved field's magnitude (max |W_gpu - W_ref| / max |W_ref| per
+component) after 10 steps; diagnostics to 1e-10 relative.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+import gks_ic
+
+pytestmark = pytest.mark.gpu
+
+STEP_RTOL = 1e-12
+STATS_RTOL = 1e-10
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def field_err(a, b):
+    """Per-component max abs difference relative to the component's scale."""
+    a = a.reshape(5, -1)
+    b = b.reshape(5, -1)
+    return np.abs(a - b).max(1) / np.abs(b).max(1)
+
+
+def interior(W):
+    return W[:, 3:-3, 3:-3, 3:-3]
+
+
+def case16(g):
+    class C:
+        pass
+
+    c = C()
+    c.nc, c.gam, c.rho0, c.Mt, c.mu0, c.p0, c.t0 = 16, 1.4, 1.0, float(g["Mt"]), float(g["mu0"]), float(g["p0"]), float(g["t0"])
+    c.K = 2
+    c.T0 = c.p0 / (287.0 * c.rho0)
+    return c
+
+
+def test_timestep_is_bitwise_reference(gks):
+    g = load("dhit16.npz")
+    with gks.Solver(gks.phys_from_case(case16(g))) as s:
+        s.upload(gks_ic.pad_periodic(g["ic"]))
+        assert s.timestep(0.5) == float(g["dt"])
+        assert s.timestep(0.02) == float(g["dt_ref_cfl"])
+
+
+def test_fp64_step_matches_reference_16(gks):
+    g = load("dhit16.npz")
+    with gks.Solver(gks.phys_from_case(case16(g))) as s:
+        s.upload(gks_ic.pad_periodic(g["ic"]))
+        s.set_dt(float(g["dt"]))
+        s.step(1)
+        s.sync()
+        e1 = field_err(interior(s.download()), g["w1"])
+        s.step(9)
+        s.sync()
+        W = s.download()
+    e10 = field_err(interior(W), g["w10"])
+    assert np.all(e1 < STEP_RTOL), e1
+    assert np.all(e10 < STEP_RTOL), e10
+    # ghosts are the periodic image
+    assert np.array_equal(W, gks_ic.pad_periodic(np.ascontiguousarray(interior(W))))
+
+
+def test_fp64_step_matches_reference_32(gks, oracle):
+    """The CPU configuration (32^3, k0 4, Mt 0.3, Re 72, seed 0): 10 steps."""
+    g = load("dhit32.npz")
+    case = gks_ic.make_dhit(32, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=0)
+    W0 = gks_ic.to_conservative_padded(case)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W0)
+        dt = s.timestep(0.5)
+        assert dt == float(g["dt"])
+        s.step(10)
+        s.sync()
+        W = interior(s.download()).reshape(5, -1)
+    ref = g["sample_w10"]
+    e = np.abs(W[:, g["sample_idx"]] - ref).max(1) / np.abs(ref).max(1)
+    assert np.all(e < STEP_RTOL), e
+    # and the whole field against the oracle
+    prm = oracle.params(32, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    Wo = W0.copy()
+    oracle.step(Wo, prm, dt, 10)
+    assert np.all(field_err(W, interior(Wo)) < STEP_RTOL)
+
+
+def test_stats_history_matches_reference_16(gks):
+    g = load("dhit16.npz")
+    with gks.Solver(gks.phys_from_case(case16(g))) as s:
+        s.upload(gks_ic.pad_periodic(g["ic"]))
+        s.set_dt(float(g["dt"]))
+        for k in range(11):
+            st = s.stats_array()
+            ref = g["stats"][k][1:9]
+            np.testing.assert_allclose(st[:8], ref, rtol=STATS_RTOL, atol=0)
+            s.step(1)
+
+
+def test_stats_match_oracle_all_columns(gks, oracle):
+    case = gks_ic.make_dhit(20, k0=4.0, Mt=0.4, Re_lambda=80.0, seed=4)
+    W = gks_ic.to_conservative_padded(case)
+    prm = oracle.params(20, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W)
+        dt = s.timestep(0.5)
+        s.step(4)
+        got = s.stats_array()
+    oracle.step(W, prm, dt, 4)
+    ref = oracle.stats(W, prm)
+    np.testing.assert_allclose(got, ref, rtol=STATS_RTOL, atol=1e-300)
+
+
+@pytest.mark.parametrize("variant", ["fix_zsweep", "direct_energy", "gpu_prandtl", "power_law"])
+def test_variants_match_oracle(gks, oracle, variant):
+    case = gks_ic.make_dhit(16, k0=4.0, Mt=0.5, Re_lambda=60.0, seed=9)
+    W = gks_ic.to_conservative_padded(case)
+    flags, oflags, law, prf = 0, 0, gks.VISC_SUTHERLAND, gks.PR_FACTOR_CPU
+    if variant == "fix_zsweep":
+        flags, oflags = gks.FIX_ZSWEEP, oracle.FIX_ZSWEEP
+    elif variant == "direct_energy":
+        flags, oflags = gks.DIRECT_ENERGY, oracle.DIRECT_ENERGY
+    elif variant == "gpu_prandtl":
+        prf = gks.PR_FACTOR_GPU
+    else:
+        law = gks.VISC_POWER
+    phys = gks.phys_from_case(case, visc_law=law, visc_exp=0.76, pr_factor=prf)
+    prm = oracle.params(16, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0, visc_law=law, visc_exp=0.76,
+                        pr_factor=prf, flags=oflags)
+    with gks.Solver(phys, gks.FP64, flags) as s:
+        s.upload(W)
+        dt = s.timestep(0.5)
+        s.step(3)
+        s.sync()
+        got = interior(s.download())
+    oracle.step(W, prm, dt, 3)
+    assert np.all(field_err(got, interior(W)) < STEP_RTOL)
+
+
+def test_zsweep_fix_changes_the_answer(gks):
+    case = gks_ic.make_dhit(16, k0=4.0, Mt=0.5, seed=9)
+    W = gks_ic.to_conservative_padded(case)
+    out = []
+    for flags in (0, gks.FIX_ZSWEEP):
+        with gks.Solver(gks.phys_from_case(case), gks.FP64, flags) as s:
+            s.upload(W)
+            s.timestep(0.5)
+            s.step(2)
+            s.sync()
+            out.append(s.download())
+    assert field_err(out[0], out[1]).max() > 1e-8
+
+
+def test_conservation_fp64_and_mixed(gks):
+    case = gks_ic.make_dhit(24, k0=4.0, Mt=0.5, seed=2)
+    W = gks_ic.to_conservative_padded(case)
+    s0 = interior(W).reshape(5, -1).sum(1)
+    scale = np.abs(interior(W)).reshape(5, -1).sum(1)
+    for prec in (gks.FP64, gks.MIXED):
+        with gks.Solver(gks.phys_from_case(case), prec) as s:
+            s.upload(W)
+            s.timestep(0.5)
+            s.step(20)
+            s.sync()
+            s1 = interior(s.download()).reshape(5, -1).sum(1)
+        assert np.all(np.abs(s1 - s0) <= 1e-12 * scale), (prec, np.abs(s1 - s0) / scale)
+
+
+def test_rest_state_stays_at_rest(gks):
+    case = gks_ic.make_dhit(8, seed=0)
+    W = np.zeros((5, 14, 14, 14))
+    W[0] = 1.0
+    W[4] = (1 / 1.4) / 0.4
+    for prec in (gks.FP64, gks.MIXED):
+        with gks.Solver(gks.phys_from_case(case), prec) as s:
+            s.upload(W)
+            s.set_dt(0.05)
+            s.step(3)
+            s.sync()
+            np.testing.assert_allclose(s.download(), W, rtol=0, atol=1e-15)
+
+
+def test_ensemble_equals_individual_runs(gks):
+    """Fields of different sizes in one context advance exactly as alone."""
+    cases = [gks_ic.make_dhit(n, k0=4.0, Mt=m, seed=sd) for n, m, sd in ((12, 0.3, 1), (16, 0.4, 2), (20, 0.2, 3))]
+    for prec in (gks.FP64, gks.MIXED):
+        alone = []
+        dts = []
+        for c in cases:
+            with gks.Solver(gks.phys_from_case(c), prec) as s:
+                s.upload(gks_ic.to_conservative_padded(c))
+                dts.append(s.timestep(0.5))
+                s.step(4)
+                s.sync()
+                alone.append(s.download())
+        with gks.Solver([gks.phys_from_case(c) for c in cases], prec) as s:
+            for f, c in enumerate(cases):
+                s.upload(gks_ic.to_conservative_padded(c), f)
+                assert s.timestep(0.5, f) == dts[f]
+            s.step(4)
+            s.sync()
+            for f in range(len(cases)):
+                assert np.array_equal(s.download(f), alone[f])
+
+
+def test_mixed_tracks_fp64(gks):
+    case = gks_ic.make_dhit(32, k0=4.0, Mt=0.5, Re_lambda=100.0, seed=0)
+    W = gks_ic.to_conservative_padded(case)
+    res = {}
+    for prec in (gks.FP64, gks.MIXED):
+        with gks.Solver(gks.phys_from_case(case), prec) as s:
+            s.upload(W)
+            s.timestep(0.5)
+            s.step(20)
+            s.sync()
+            res[prec] = (s.download(), s.stats())
+    e = field_err(res[gks.MIXED][0], res[gks.FP64][0])
+    assert np.all(e < 1e-6), e
+    for key in ("tke", "diss"):
+        a, b = res[gks.MIXED][1][key], res[gks.FP64][1][key]
+        assert abs(a - b) < 1e-5 * abs(b), (key, a, b)
+
+
+def test_nonfinite_state_is_reported(gks):
+    case = gks_ic.make_dhit(8, seed=0)
+    W = gks_ic.to_conservative_padded(case)
+    W[0, 5, 5, 5] = np.nan
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W)
+        with pytest.raises(gks.GksError) as ei:
+            s.check()
+        assert ei.value.code == -5
+
+
+def test_call_order_is_enforced(gks):
+    case = gks_ic.make_dhit(8, seed=0)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        with pytest.raises(gks.GksError) as ei:
+            s.step(1)
+        assert ei.value.code == -4
+        s.upload(gks_ic.to_conservative_padded(case))
+        with pytest.raises(gks.GksError):
+            s.step(1)  # no dt yet
+        with pytest.raises(gks.GksError):
+            s.set_dt(-1.0)
+        with pytest.raises(ValueError):
+            s.upload(np.zeros((5, 10, 10, 10)))
