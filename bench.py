@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark of the GKM-DNS WENO-GKS step on B200.
+
+Workload: one decaying-isotropic-turbulence field at 256^3 (k0 4, Mt 0.5,
+Re_lambda 100, CFL 0.5, seeded synthetic initial field; the configuration the
+headline metric is quoted on).  A step is one pass of the hot path: the three
+reconstruction + flux sweeps and the conservative update.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours       K timed steps of the FP64 path (the parity path, `value`) and of the
+           mixed FP32/FP64 path (`mixed`), state resident in HBM (671 MB per
+           field, above the 126 MB L2, so no flush between steps); CUDA events
+           on the library's stream; max over ranks.  `e2e` times the
+           reference-facing call (upload from pinned host memory, one step,
+           download) per step.  `roofline` is the dominant kernel (the flux
+           sweep) timed live with CUDA events against the FP64 FMA peak
+           measured live on the same GPU.  Under torchrun every rank advances
+           its own replica (replicas only: the path does not shard).
+reference  the reference's own CPU implementation (oracle/_ref, compiled from
+           its sources) on the host cores: one process per core (at most 64),
+           each timing the reference step on a 2-plane y-slab of the same
+           256^3 field (about 1 s of CPU per step and process).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gkm-dns_b200"))
+
+METRIC = "cell-updates/s at 256³, FP64 vs mixed FP32/FP64 (err vs FP64); HBM GB/s"
+UNIT = "cell-updates/s"
+NC = 256
+K0, MACH, RE = 4.0, 0.5, 100.0
+CFL = 0.5
+# Algorithmic work (reference operation counts of flux() and ApplyWENO(), one
+# WENO per line and interface): FP64 operations per interface in the flux
+# kernel (flux 8005 + slopes 90 + c2p/viscosity/tau 25) and in the
+# reconstruction kernel (5-component WENO 1122); per cell-update 3 interfaces
+# + 30 for the update.
+OPS_FLUX = 8005 + 90 + 25
+OPS_RECON = 1122
+OPS_CELL = 3 * (OPS_FLUX + OPS_RECON) + 30
+BYTES_CELL = 80  # 5 doubles read + 5 written per cell-update
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    def __init__(self, ws, local):
+        self.ws = ws
+        self.pg = None
+        if ws > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, pw, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+                pw.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "power_w_max": max(pw) if pw else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def gpu_uuid(local: int) -> str:
+    try:
+        import torch
+
+        u = torch.cuda.get_device_properties(local).uuid
+        return "GPU-" + str(u)
+    except Exception:
+        return str(local)
+
+
+def read_traffic(nc: int):
+    """DRAM bytes per flux launch from the committed ncu summary, scaled to nc^3 cells."""
+    path = os.path.join(ROOT, "profiles", "flux_fp64_ncu.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_interface"):
+                    return float(line.split("=")[1].split()[0]) * nc ** 3
+    except OSError:
+        pass
+    return None
+
+
+def make_case(nc: int, seed: int):
+    import gks_ic
+
+    return gks_ic.make_dhit(nc, k0=K0, Mt=MACH, Re_lambda=RE, seed=seed)
+
+
+def timed_steps(solver, steps: int, torch) -> float:
+    """ms per step over `steps` graph launches, CUDA events on the library stream."""
+    stream = torch.cuda.ExternalStream(solver.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    solver.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    solver.sync()
+    return e0.elapsed_time(e1) / steps
+
+
+def cpu_baseline(nc: int, steps: int, warmup: int, planes: int = 8, procs: int = 1) -> dict | None:
+    """The reference CPU step (oracle/_ref) on y-slabs of the same field."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gks_ic
+    import pyoracle
+
+    if not os.path.exists(pyoracle.REF_HARNESS_FAST):
+        return None
+    case = make_case(nc, 0)
+    d = tempfile.mkdtemp(prefix="gks_cpu_")
+    gks_ic.write_case(d, case, slab_planes=planes)
+    cmd = pyoracle.ref_time_cmd(d, steps, nc // planes, CFL, warmup)
+    ps = [subprocess.Popen(cmd, stdout=subprocess.PIPE, text=True) for _ in range(procs)]
+    res = []
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            return None
+        res.append(json.loads(out.strip().splitlines()[-1]))
+    secs = max(r["seconds"] for r in res)
+    cells = sum(r["cells"] for r in res)
+    return {"value": cells * steps / secs, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{steps} timed step(s) after {warmup} warm-up of the reference CPU step "
+                      f"(update.cpp evolveEulerian + HaloTransfer, g++ -O3 -march=x86-64-v3) on a "
+                      f"{planes}x{nc}x{nc} y-slab of the {nc}^3 field per process, {procs} process(es)"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    procs = max(1, min(len(os.sched_getaffinity(0)), 64))
+    warm, steps = max(0, args.warmup), max(1, args.steps)
+    cb = cpu_baseline(NC, steps, warm, planes=2, procs=procs)
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness_fast is not built"}))
+        return 0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": 0,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * NC ** 3 / cb["value"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"DHIT {NC}^3 WENO-GKS step (FP64), reference CPU path",
+                   "nc": NC, "k0": K0, "mach_t": MACH, "re_lambda": RE, "cfl": CFL},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import gks_b200 as gks
+    import gks_ic
+
+    ws, rank, local = dist_env()
+    dist = Dist(ws, local)
+    torch.cuda.set_device(local)
+    gks.select_device(local)
+    nc = args.nc
+    case = make_case(nc, rank)
+    W = gks_ic.to_conservative_padded(case)
+    phys = gks.phys_from_case(case)
+    uuid = gpu_uuid(local)
+
+    # peaks of the FP64 / FP32 pipes, measured here (no FP64 figure is supplied)
+    peak64 = gks.peak_tflops(gks.FP64)
+    peak32 = gks.peak_tflops(gks.MIXED)
+
+    results = {}
+    solvers = {}
+    for name, prec in (("fp64", gks.FP64), ("mixed", gks.MIXED)):
+        s = gks.Solver(phys, prec, device=local)
+        s.upload(W)
+        dt = s.timestep(CFL)
+        s.step(args.warmup)
+        s.sync()
+        dist.barrier()
+        sampler = ClockSampler(uuid) if name == "fp64" else None
+        if sampler:
+            sampler.start()
+        ms = timed_steps(s, args.steps, torch)
+        clocks = sampler.stop() if sampler else None
+        ms = dist.max(ms)
+        results[name] = {"ms": ms, "dt": dt, "clocks": clocks, "stats": s.stats()}
+        solvers[name] = s
+
+    # stage timing (CUDA events around every launch) on both paths
+    stages = {name: solvers[name].time_stages(3) for name in solvers}
+    for name in solvers:
+        solvers[name].close()
+
+    # e2e through the reference-facing call: upload from pinned host, step, download
+    nt = nc + 6
+    host = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True).numpy()
+    host[...] = W
+    s = gks.Solver(phys, gks.FP64, device=local)
+    s.upload(host)
+    s.timestep(CFL)
+    stream = torch.cuda.ExternalStream(s.stream())
+    e2e_steps = max(1, min(args.steps, 5))
+    s.upload(host); s.step(1); s.download(out=host)  # warm-up of the copy path
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s.upload(host)
+        s.step(1)
+        s.download(out=host)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = dist.max(e0.elapsed_time(e1) / e2e_steps)
+    s.close()
+    bytes_io = 5 * nt ** 3 * 8
+
+    cells = nc ** 3
+    value = ws * cells / (results["fp64"]["ms"] * 1e-3)
+    mixed_value = ws * cells / (results["mixed"]["ms"] * 1e-3)
+    flux_ms = statistics.mean(stages["fp64"][k] for k in ("flux_x", "flux_y", "flux_z"))
+    recon_ms = statistics.mean(stages["fp64"][k] for k in ("recon_x", "recon_y", "recon_z"))
+    achieved = OPS_FLUX * cells / (flux_ms * 1e-3) / 1e12
+    traffic = read_traffic(nc)
+    st64, st32 = results["fp64"]["stats"], results["mixed"]["stats"]
+    rel = {k: abs(st32[k] - st64[k]) / abs(st64[k]) for k in ("tke", "diss", "skew_u", "skew_v", "skew_w")}
+
+    cb = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cb = cpu_baseline(nc, 1, 1, planes=8, procs=1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": results["fp64"]["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded solenoidal DHIT field (k0 4, Mt 0.5, Re_lambda 100), one replica per GPU",
+            "config": {"workload": f"DHIT {nc}^3 WENO-GKS step, FP64 parity path", "nc": nc, "k0": K0,
+                       "mach_t": MACH, "re_lambda": RE, "cfl": CFL, "precision": "fp64",
+                       "parallelism": f"replicas x{ws}", "l2": "state 671 MB per field > 126 MB L2, no flush"},
+            "mixed": {"value": mixed_value, "ms_per_step": results["mixed"]["ms"],
+                      "speedup_vs_fp64": mixed_value / value,
+                      "rel_err_vs_fp64_after_steps": rel, "steps_compared": args.warmup + args.steps,
+                      "dtype": "f32 weno/slopes/slope moments + f64 moments/erfc/update/reductions",
+                      "stage_ms": stages["mixed"]},
+            "roofline": {"bound": "fp64", "kernel": "flux sweep (k_flux, FP64)", "achieved": achieved,
+                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": traffic,
+                         "peak_source": "FP64 FMA peak measured live by gks_peak_flops on this GPU",
+                         "ops_per_interface": OPS_FLUX, "launch_ms": flux_ms,
+                         "step_achieved": OPS_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e12,
+                         "fp32_peak": peak32},
+            "hbm": {"achieved_gbs": BYTES_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e9,
+                    "peak_gbs": 6538.0, "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
+            "stage_ms": stages["fp64"], "recon_ms": recon_ms,
+            "e2e": {"value": ws * cells / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+                    "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms,
+                    "call": "gks_upload + gks_step(1) + gks_download per step, pinned host buffers"},
+            "clocks": results["fp64"]["clocks"],
+            "gpu_launches": 7 * args.steps,
+        }
+        if cb:
+            line["cpu_baseline"] = cb
+        print(json.dumps(line))
+    dist.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nc", type=int, default=NC)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("at least 3 warm-up steps")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

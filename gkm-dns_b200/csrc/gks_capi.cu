@@ -469,6 +469,46 @@ int gks_set_stream(gks_ctx *ctx, void *stream)
     return GKS_OK;
 }
 
+int gks_select_device(int device)
+{
+    return cudaSetDevice(device) == cudaSuccess ? GKS_OK : GKS_ECUDA;
+}
+
+int gks_time_stages(gks_ctx *ctx, int reps, double *ms)
+{
+    if (!ctx || !ms || reps < 1) return GKS_EINVAL;
+    for (int f = 0; f < ctx->nfields; ++f)
+        if (!ctx->fh[f].uploaded || !ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "time_stages before upload/dt");
+    CK(cudaSetDevice(ctx->device));
+    cudaEvent_t ev[8];
+    for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&ev[i]));
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    int rc = GKS_OK;
+    for (int r = 0; r < reps && rc == GKS_OK; ++r) {
+        cudaError_t e = cudaEventRecord(ev[0], ctx->stream);
+        for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) {
+            e = gks::launch_recon(ctx->batch, dir, ctx->precision, ctx->cfg[gks::K_RECON][dir], ctx->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[2 * dir + 1], ctx->stream);
+            if (e == cudaSuccess)
+                e = gks::launch_flux(ctx->batch, dir, ctx->precision, ctx->cfg[gks::K_FLUX][dir], ctx->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[2 * dir + 2], ctx->stream);
+        }
+        if (e == cudaSuccess) e = gks::launch_update(ctx->batch, ctx->cfg[gks::K_UPDATE][0], ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[7], ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[7]);
+        for (int i = 0; i < 7 && e == cudaSuccess; ++i) {
+            float t = 0;
+            e = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+            acc[i] += t;
+        }
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "stage timing");
+    }
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
+    if (rc) return rc;
+    for (int i = 0; i < 7; ++i) ms[i] = acc[i] / reps;
+    return GKS_OK;
+}
+
 int gks_get_stream(gks_ctx *ctx, void **stream)
 {
     if (!ctx || !stream) return GKS_EINVAL;

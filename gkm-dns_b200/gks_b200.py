@@ -83,7 +83,27 @@ SIGNATURES = {
     "gks_device_fields": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
     "gks_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "gks_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "gks_select_device": (ctypes.c_int, [ctypes.c_int]),
+    "gks_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP]),
+    "gks_peak_flops": (ctypes.c_int, [ctypes.c_int, DP]),
 }
+
+STAGES = ["recon_x", "flux_x", "recon_y", "flux_y", "recon_z", "flux_z", "update"]
+
+
+def select_device(device: int) -> None:
+    rc = load_library().gks_select_device(device)
+    if rc != 0:
+        raise GksError(rc, f"cannot select CUDA device {device}")
+
+
+def peak_tflops(precision: int = FP64) -> float:
+    """Measured FMA peak of the current device's FP64 (FP64) or FP32 (MIXED) pipe."""
+    out = ctypes.c_double()
+    rc = load_library().gks_peak_flops(precision, ctypes.byref(out))
+    if rc != 0:
+        raise GksError(rc, "peak measurement failed")
+    return out.value
 
 _lib = None
 
@@ -124,8 +144,10 @@ class _Field:
 class Solver:
     """One context on the current CUDA device holding one or more fields."""
 
-    def __init__(self, phys, precision: int = FP64, flags: int = 0):
+    def __init__(self, phys, precision: int = FP64, flags: int = 0, device: int | None = None):
         lib = load_library()
+        if device is not None:
+            select_device(device)
         if isinstance(phys, Phys):
             phys = [phys]
         arr = (Phys * len(phys))(*phys)
@@ -213,6 +235,12 @@ class Solver:
         s = ctypes.c_void_p()
         self._ck(self._lib.gks_get_stream(self._h, ctypes.byref(s)))
         return s.value or 0
+
+    def time_stages(self, reps: int = 3) -> dict:
+        """Mean ms per stage over reps individually launched steps (advances the state)."""
+        ms = (ctypes.c_double * 7)()
+        self._ck(self._lib.gks_time_stages(self._h, reps, ms))
+        return dict(zip(STAGES, list(ms)))
 
     def set_stream(self, stream: int | None):
         self._ck(self._lib.gks_set_stream(self._h, ctypes.c_void_p(stream or 0)))

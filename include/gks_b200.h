@@ -137,6 +137,19 @@ int gks_set_stream(gks_ctx *ctx, void *stream);
 /* The cudaStream_t the context launches on (for event timing by callers). */
 int gks_get_stream(gks_ctx *ctx, void **stream);
 
+/* Make `device` the calling thread's CUDA device for this library (contexts
+ * are created on the device current at gks_create). */
+int gks_select_device(int device);
+
+/* Advance reps steps launching the seven stages one by one with CUDA events
+ * between them; ms[0..6] receives the mean time of recon x, flux x, recon y,
+ * flux y, recon z, flux z, update.  For profiling: the state advances. */
+int gks_time_stages(gks_ctx *ctx, int reps, double *ms);
+
+/* Peak FMA throughput of the FP64 (GKS_FP64) or FP32 (GKS_MIXED) pipe of
+ * the current device in TFLOP/s, 2 flops per FMA (a short microbenchmark). */
+int gks_peak_flops(int precision, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -182,9 +182,13 @@ def ref_flux(inputs: np.ndarray, gam=1.4, K=2):
     return np.fromfile(os.path.join(d, "out"), dtype=np.float64).reshape(n, 5)
 
 
-def ref_time(casedir: str, nsteps: int, slabs: int, cfl: float, fast=True) -> dict:
-    import json
+def ref_time_cmd(casedir: str, nsteps: int, slabs: int, cfl: float, warmup: int = 0, fast=True) -> list:
     exe = REF_HARNESS_FAST if fast else REF_HARNESS
-    cp = subprocess.run([exe, "time", os.path.abspath(casedir), str(nsteps), str(slabs), repr(cfl)],
-                        check=True, capture_output=True, text=True)
+    return [exe, "time", os.path.abspath(casedir), str(nsteps), str(slabs), repr(cfl), str(warmup)]
+
+
+def ref_time(casedir: str, nsteps: int, slabs: int, cfl: float, warmup: int = 0, fast=True) -> dict:
+    import json
+    cp = subprocess.run(ref_time_cmd(casedir, nsteps, slabs, cfl, warmup, fast), check=True, capture_output=True,
+                        text=True)
     return json.loads(cp.stdout.strip().splitlines()[-1])

@@ -20,9 +20,9 @@
  *        dt = cfl*dx/maxVAL with maxVAL from the reference's timestep().
  *        Writes W_<step>.bin (5 padded arrays), stats.bin (per stats call:
  *        t/t0 TKE Diss SKEWu SKEWv SKEWw KURTu KURTv KURTw), meta.txt.
- *   time <casedir> <nsteps> <slabs> <cfl>
+ *   time <casedir> <nsteps> <slabs> <cfl> [warmup]
  *        Times evolveEulerian + HaloTransfer on the y-slab 0 of a <slabs>x1x1
- *        process grid; prints one JSON line.
+ *        process grid after [warmup] untimed steps; prints one JSON line.
  *   weno <in> <out>   ApplyWENO (update.cpp:502-625) on packed stencils.
  *   flux <in> <out>   flux (GKMflux.cpp:11-215) on packed interface states.
  */
@@ -171,10 +171,11 @@ int mode_run(int argc, char **argv)
 
 int mode_time(int argc, char **argv)
 {
-    if (argc < 6) { fprintf(stderr, "time <casedir> <nsteps> <slabs> <cfl>\n"); return 2; }
+    if (argc < 6) { fprintf(stderr, "time <casedir> <nsteps> <slabs> <cfl> [warmup]\n"); return 2; }
     const int nsteps = atoi(argv[3]);
     const int slabs = atoi(argv[4]);
     const double cfl_run = atof(argv[5]);
+    const int warmup = argc > 6 ? atoi(argv[6]) : 0;
     if (chdir(argv[2]) != 0) { perror("chdir"); return 2; }
     setup_block(slabs);
     ptype *W[5], *Fx[5], *Fy[5], *Fz[5];
@@ -190,6 +191,10 @@ int mode_time(int argc, char **argv)
     halo.exchange(W);
     timestep(W);
     if (cfl_run > 0) dt = cfl_run * dx / maxVAL;
+    for (int s = 0; s < warmup; ++s) {
+        evolveEulerian(W, Fx, Fy, Fz);
+        halo.exchange(W);
+    }
     std::vector<double> secs;
     for (int s = 0; s < nsteps; ++s) {
         auto a = std::chrono::steady_clock::now();
