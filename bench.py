@@ -264,6 +264,8 @@ def run_ours(args):
         s = gks.Solver(phys, prec, device=local)
         s.upload(W)
         dt = s.timestep(CFL)
+        if not args.no_tune:
+            s.autotune(2)
         s.step(args.warmup)
         s.sync()
         dist.barrier()
@@ -273,7 +275,7 @@ def run_ours(args):
         ms = timed_steps(s, args.steps, torch)
         clocks = sampler.stop() if sampler else None
         ms = dist.max(ms)
-        results[name] = {"ms": ms, "dt": dt, "clocks": clocks, "stats": s.stats()}
+        results[name] = {"ms": ms, "dt": dt, "clocks": clocks, "stats": s.stats(), "launch": s.launch_config()}
         solvers[name] = s
 
     # stage timing (CUDA events around every launch) on both paths
@@ -343,6 +345,8 @@ def run_ours(args):
             "hbm": {"achieved_gbs": BYTES_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e9,
                     "peak_gbs": 6538.0, "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
             "stage_ms": stages["fp64"], "recon_ms": recon_ms,
+            "launch": {"fp64": results["fp64"]["launch"], "mixed": results["mixed"]["launch"],
+                       "tuned": not args.no_tune},
             "e2e": {"value": ws * cells / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms,
                     "call": "gks_upload + gks_step(1) + gks_download per step, pinned host buffers"},
@@ -364,6 +368,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--nc", type=int, default=NC)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-tune", action="store_true", help="keep the untuned launch configuration")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("at least 3 warm-up steps")

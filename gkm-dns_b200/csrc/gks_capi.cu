@@ -11,9 +11,13 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -134,23 +138,48 @@ int read_err(gks_ctx *ctx, int *word, bool clear)
     return GKS_OK;
 }
 
+// Persistent grid: `mult` times the resident blocks of the kernel, no more
+// blocks than the work needs.
+gks::LaunchCfg persistent(gks_ctx *ctx, int kind, int dir, int variant, int mult)
+{
+    gks::LaunchCfg c;
+    c.block = kind == gks::K_UPDATE ? 256 : 128;
+    c.variant = variant;
+    int per_sm = 1;
+    if (gks::max_resident_blocks(kind, dir, ctx->precision, variant, c.block, &per_sm) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    long long g = (long long)ctx->nsm * per_sm * mult;
+    const long long need = (ctx->batch.total + c.block - 1) / c.block;
+    if (g > need) g = need;
+    if (g < 1) g = 1;
+    c.grid = (int)g;
+    return c;
+}
+
+// Untuned defaults: the mixed flux at the 168-register cap (its spill is
+// negligible there), everything else uncapped.
 void choose_launch(gks_ctx *ctx)
 {
-    // persistent grids: every SM filled to its occupancy limit, no more blocks than work
-    const long long total = ctx->batch.total;
     for (int kind = 0; kind < gks::K_KINDS; ++kind)
         for (int dir = 0; dir < 3; ++dir) {
-            const int block = kind == gks::K_UPDATE ? 256 : 128;
-            int per_sm = 1;
-            if (gks::max_resident_blocks(kind, dir, ctx->precision, block, &per_sm) != cudaSuccess || per_sm < 1)
-                per_sm = 1;
-            long long g = (long long)ctx->nsm * per_sm;
-            const long long need = (total + block - 1) / block;
-            if (g > need) g = need;
-            if (g < 1) g = 1;
-            ctx->cfg[kind][dir].block = block;
-            ctx->cfg[kind][dir].grid = (int)g;
+            const int variant = (kind == gks::K_FLUX && ctx->precision == GKS_MIXED) ? 1 : 0;
+            ctx->cfg[kind][dir] = persistent(ctx, kind, dir, variant, 1);
         }
+}
+
+// Tuned configurations of this process, per device / precision / flags / sizes.
+std::mutex g_tune_mu;
+std::map<std::string, std::array<gks::LaunchCfg, gks::K_KINDS * 3>> g_tune_cache;
+
+std::string tune_key(const gks_ctx *ctx)
+{
+    std::vector<int> ns;
+    for (const FieldHost &h : ctx->fh) ns.push_back(h.phys.nc);
+    std::sort(ns.begin(), ns.end());
+    std::string k = "d" + std::to_string(ctx->device) + "p" + std::to_string(ctx->precision) + "f" +
+                    std::to_string(ctx->flags) + ":";
+    for (int n : ns) k += std::to_string(n) + ",";
+    return k;
 }
 
 int record_step(gks_ctx *ctx)
@@ -195,7 +224,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     if (flags & ~(GKS_FIX_ZSWEEP | GKS_DIRECT_ENERGY)) return GKS_EINVAL;
     for (int f = 0; f < nfields; ++f) {
         const gks_phys &p = phys[f];
-        if (p.nc < 4 || p.nc > 4096 || !(p.gam > 1.0) || !(p.R > 0) || !(p.T0 > 0) || !(p.mu0 >= 0) ||
+        if (p.nc < 4 || p.nc > 4096 || !(p.gam > 1.0) || !(p.gas_r > 0) || !(p.T0 > 0) || !(p.mu0 >= 0) ||
             p.K < 0 || (p.visc_law != GKS_VISC_SUTHERLAND && p.visc_law != GKS_VISC_POWER) || !(p.pr_factor > 0))
             return GKS_EINVAL;
     }
@@ -249,9 +278,9 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.dt = 0.0;
         d.gam = p.gam;
         d.gm1 = p.gam - 1;
-        d.R = p.R;
-        d.cT = (p.gam - 1) / p.R;
-        d.icT = p.R / (p.gam - 1.0);
+        d.R = p.gas_r;
+        d.cT = (p.gam - 1) / p.gas_r;
+        d.icT = p.gas_r / (p.gam - 1.0);
         d.T0 = p.T0;
         d.iT0 = 1.0 / p.T0;
         d.mu0 = p.mu0;
@@ -506,6 +535,93 @@ int gks_time_stages(gks_ctx *ctx, int reps, double *ms)
     for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
     if (rc) return rc;
     for (int i = 0; i < 7; ++i) ms[i] = acc[i] / reps;
+    return GKS_OK;
+}
+
+int gks_autotune(gks_ctx *ctx, int reps)
+{
+    if (!ctx || reps < 1) return GKS_EINVAL;
+    for (int f = 0; f < ctx->nfields; ++f)
+        if (!ctx->fh[f].uploaded || !ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "autotune before upload/dt");
+    CK(cudaSetDevice(ctx->device));
+    const std::string key = tune_key(ctx);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            for (int i = 0; i < gks::K_KINDS * 3; ++i) ctx->cfg[i / 3][i % 3] = it->second[i];
+            drop_graph(ctx);
+            return GKS_OK;
+        }
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int rc = GKS_OK;
+    // time `reps` launches of one candidate after one untimed launch; the
+    // reconstruction and flux kernels only write scratch, so repeating them
+    // leaves the state unchanged (the update is not tuned for that reason)
+    auto time_it = [&](int kind, int dir, gks::LaunchCfg c, float *ms) -> cudaError_t {
+        auto go = [&]() {
+            return kind == gks::K_RECON ? gks::launch_recon(ctx->batch, dir, ctx->precision, c, ctx->stream)
+                                        : gks::launch_flux(ctx->batch, dir, ctx->precision, c, ctx->stream);
+        };
+        cudaError_t e = go();
+        if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < reps && e == cudaSuccess; ++r) e = go();
+        if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+        return e;
+    };
+    const int mults[2] = {1, 2};
+    for (int dir = 0; dir < 3 && rc == GKS_OK; ++dir) {
+        for (int kind : {int(gks::K_RECON), int(gks::K_FLUX)}) {
+            const int nvar = kind == gks::K_RECON ? gks::kReconVariants : gks::kFluxVariants;
+            float best = 1e30f;
+            gks::LaunchCfg bestc = ctx->cfg[kind][dir];
+            for (int v = 0; v < nvar && rc == GKS_OK; ++v)
+                for (int m : mults) {
+                    const gks::LaunchCfg c = persistent(ctx, kind, dir, v, m);
+                    float ms = 0;
+                    const cudaError_t e = time_it(kind, dir, c, &ms);
+                    if (e != cudaSuccess) {
+                        rc = cuda_fail(ctx, e, "autotune");
+                        break;
+                    }
+                    if (ms < best) {
+                        best = ms;
+                        bestc = c;
+                    }
+                }
+            ctx->cfg[kind][dir] = bestc;
+            // leave this sweep's reconstruction in place for timing its flux
+            if (rc == GKS_OK && kind == gks::K_RECON) {
+                const cudaError_t e = gks::launch_recon(ctx->batch, dir, ctx->precision, bestc, ctx->stream);
+                if (e != cudaSuccess) rc = cuda_fail(ctx, e, "autotune");
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    std::array<gks::LaunchCfg, gks::K_KINDS * 3> a;
+    for (int i = 0; i < gks::K_KINDS * 3; ++i) a[i] = ctx->cfg[i / 3][i % 3];
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = a;
+    }
+    drop_graph(ctx);
+    return GKS_OK;
+}
+
+int gks_get_launch(gks_ctx *ctx, int kind, int dir, int *block, int *grid, int *variant)
+{
+    if (!ctx || kind < 0 || kind >= gks::K_KINDS || dir < 0 || dir > 2) return GKS_EINVAL;
+    const gks::LaunchCfg &c = ctx->cfg[kind][dir];
+    if (block) *block = c.block;
+    if (grid) *grid = c.grid;
+    if (variant) *variant = c.variant;
     return GKS_OK;
 }
 

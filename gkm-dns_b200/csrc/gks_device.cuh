@@ -234,19 +234,18 @@ __device__ __forceinline__ void cast5(S out[5], const double in[5])
 
 // ---------------------------------------------------------------------------
 // Time-integrated BGK-NS interface flux (GKMflux.cpp:11-215), in the frame of
-// the interface normal.  Inputs: cell states WL, WR either side, reconstructed
-// states Wl, Wr, their slopes DWl[d][q], DWr[d][q] (d = normal, first and
-// second transverse direction), the collision time tau0 = mu/p at the left
-// cell.  Output F[5] (flux integrated over [0, dt]).
+// the interface normal.  The caller supplies the inputs through `src`, which
+// is asked for them only when they are needed, so that one side's inputs are
+// not live while the other side is processed:
+//   src.state(side, W)      reconstructed state Wl (side 0) or Wr (side 1)
+//   src.slopes(side, DW)    its slopes DW[d][q], d = normal, 1st, 2nd transverse
+//   src.cells(WL, WR)       the cell averages either side of the interface
+// tau0 = mu/p at the left cell.  Output F[5], the flux integrated over [0, dt].
 // ---------------------------------------------------------------------------
-template <typename S, int NEG>
-__device__ __forceinline__ void flux_side(const Prim &g, const S DW[3][5], const FluxConst &c,
-                                          // time weights
-                                          double gmB1, double gmB2, double gmB3, // gm3, gm4+gm5, gm5
-                                          double pF3, double pF4, double pF5,   // p3, p4, p5
-                                          // accumulators
-                                          double We[5], double Bbase[5], double Fbase[5],
-                                          S by_[5], S bz_[5], S Bs[5], S Fs[5])
+template <typename S, int NEG, typename Src>
+__device__ __forceinline__ void flux_side(const Src &src, const Prim &g, const FluxConst &c,
+                                          double gmB2, double gmB3, double pF3, double pF4, double pF5,
+                                          double We[5], double Fbase[5], S by_[5], S bz_[5], S Bs[5], S Fs[5])
 {
     // tables of this Maxwellian (double): transverse Y, Z and the normal half space
     double Y[6], Z[6], X[7];
@@ -260,7 +259,7 @@ __device__ __forceinline__ void flux_side(const Prim &g, const S DW[3][5], const
         const double ex = 0.5 * exp(-g.lam * g.U0 * g.U0) * rsqrt(kPi * g.lam);
         half_table<7>(g.U0, g.s, h0, NEG ? -ex : ex, X);
     }
-    // zeroth-order moments (double): W0 contribution, B_ and F base terms
+    // zeroth-order moments (double): W0 (GKMflux.cpp:71-75) and the p3 term of F
     {
         double M0[5], M1[5];
         mcal0<0, 0, 0, double>(M0, X, Y, Z, e2);
@@ -268,7 +267,6 @@ __device__ __forceinline__ void flux_side(const Prim &g, const S DW[3][5], const
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             We[q] += g.den * M0[q];
-            Bbase[q] += gmB1 * g.den * M0[q];
             Fbase[q] += pF3 * g.den * M1[q];
         }
     }
@@ -277,6 +275,8 @@ __device__ __forceinline__ void flux_side(const Prim &g, const S DW[3][5], const
     const SlopeFrame<S> fr = slope_frame<S>(S(g.U0), S(g.U1), S(g.U2), S(g.lam), S(g.s), c.K, S(c.kA));
     S ax[5], ay[5], az[5];
     {
+        S DW[3][5];
+        src.slopes(NEG, DW);
         S b[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) b[q] = DW[0][q] * rinv;
@@ -345,13 +345,17 @@ __device__ __forceinline__ void flux_side(const Prim &g, const S DW[3][5], const
     }
 }
 
-template <typename S>
-__device__ __forceinline__ void gks_flux(const double WL[5], const double WR[5], const double Wl[5],
-                                         const double Wr[5], const S DWl[3][5], const S DWr[3][5],
-                                         double tau0, const FluxConst &c, double F[5])
+template <typename S, typename Src>
+__device__ __forceinline__ void gks_flux(const Src &src, double tau0, const FluxConst &c, double F[5])
 {
-    const Prim l = prim(Wl, c.gm1);
-    const Prim r = prim(Wr, c.gm1);
+    Prim l, r;
+    {
+        double Ws[5];
+        src.state(0, Ws);
+        l = prim(Ws, c.gm1);
+        src.state(1, Ws);
+        r = prim(Ws, c.gm1);
+    }
     // collision time with the pressure-jump term (GKMflux.cpp:149-150):
     // rho/lambda = 2p, so w = |p_l - p_r| / (p_l + p_r)
     const double dt = c.dt;
@@ -375,10 +379,10 @@ __device__ __forceinline__ void gks_flux(const double WL[5], const double WR[5],
     const double p4 = -Qt - tau * Pt;
     const double p5 = -tau * Pt;
 
-    double We[5] = {0, 0, 0, 0, 0}, Bbase[5] = {0, 0, 0, 0, 0}, Fbase[5] = {0, 0, 0, 0, 0};
+    double We[5] = {0, 0, 0, 0, 0}, Fbase[5] = {0, 0, 0, 0, 0};
     S by_[5] = {0, 0, 0, 0, 0}, bz_[5] = {0, 0, 0, 0, 0}, Bs[5] = {0, 0, 0, 0, 0}, Fs[5] = {0, 0, 0, 0, 0};
-    flux_side<S, 0>(l, DWl, c, gm3, gm4 + gm5, gm5, p3, p4, p5, We, Bbase, Fbase, by_, bz_, Bs, Fs);
-    flux_side<S, 1>(r, DWr, c, gm3, gm4 + gm5, gm5, p3, p4, p5, We, Bbase, Fbase, by_, bz_, Bs, Fs);
+    flux_side<S, 0>(src, l, c, gm4 + gm5, gm5, p3, p4, p5, We, Fbase, by_, bz_, Bs, Fs);
+    flux_side<S, 1>(src, r, c, gm4 + gm5, gm5, p3, p4, p5, We, Fbase, by_, bz_, Bs, Fs);
 
     // equilibrium state at the interface (GKMflux.cpp:71-98)
     const Prim e = prim(We, c.gm1);
@@ -389,18 +393,26 @@ __device__ __forceinline__ void gks_flux(const double WL[5], const double WR[5],
     const double e2 = double(c.K) * e.s;
     const double e4 = double(c.K * (c.K + 2)) * e.s * e.s;
     {
+        // 0.5 erfc(-+x) from one evaluation at |x|: the far tail is computed
+        // directly, the other value as 1 - tail (no cancellation)
         const double sl = sqrt(e.lam);
+        const double x = sl * e.U0;
+        const double tail = 0.5 * erfc(fabs(x));
+        const double hp = x >= 0.0 ? 1.0 - tail : tail; // 0.5 erfc(-x)
+        const double hn = x >= 0.0 ? tail : 1.0 - tail; // 0.5 erfc(x)
         const double g = 0.5 * exp(-e.lam * e.U0 * e.U0) * rsqrt(kPi * e.lam);
-        half_table<7>(e.U0, e.s, 0.5 * erfc(-sl * e.U0), g, Xp);
-        half_table<7>(e.U0, e.s, 0.5 * erfc(sl * e.U0), -g, Xn);
+        half_table<7>(e.U0, e.s, hp, g, Xp);
+        half_table<7>(e.U0, e.s, hn, -g, Xn);
     }
+    // B_ base terms: gm1 rho_e <psi>_e + gm3 W0 (GKMflux.cpp:174), nearly cancelling
+    double Bbase[5];
     {
         double M0[5], M1[5];
         mcal0<0, 0, 0, double>(M0, Xf, Y, Z, e2);
         mcal0<1, 0, 0, double>(M1, Xf, Y, Z, e2);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            Bbase[q] += gm1 * e.den * M0[q];
+            Bbase[q] = gm1 * e.den * M0[q] + gm3 * We[q];
             Fbase[q] += p0 * e.den * M1[q];
         }
     }
@@ -408,6 +420,8 @@ __device__ __forceinline__ void gks_flux(const double WL[5], const double WR[5],
     S axl[5], axr[5], ay[5], az[5];
     {
         // normal slopes of the equilibrium state from the cell averages (GKMflux.cpp:109-110)
+        double WL[5], WR[5];
+        src.cells(WL, WR);
         const double k2 = 2.0 * e.rinv * (1.0 / c.dx);
         S b[5];
 #pragma unroll

@@ -82,8 +82,8 @@ __device__ __forceinline__ double temperature(const double W[5], double cT)
 // Reconstruction: Wl, Wr at the interface between cell c and its +1
 // neighbour along DIR (update.cpp:247 / GPUupdate.cu:917-977).
 // ---------------------------------------------------------------------------
-template <int DIR, int PREC>
-__global__ void __launch_bounds__(128) k_recon(Batch b)
+template <int DIR, int PREC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_recon(Batch b)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
@@ -179,56 +179,76 @@ __device__ __forceinline__ void transverse(const Cell &x, int flags, long long &
     }
 }
 
-template <typename T>
-__device__ __forceinline__ void rot5(T v[5], int r)
-{
-    const T t = v[1];
-    v[1] = v[r];
-    v[r] = t;
-}
+// Inputs of one interface, read on demand (see gks_flux).  Slot q of the
+// rotated frame holds original component perm(q): rho v (y sweep) or rho w
+// (z sweep) moves into slot 1 (update.cpp:340-350, 429-439).
+template <int DIR, typename S>
+struct SweepSrc {
+    const FieldDev *f;
+    long long c, c1, cn, cs, cf, cb;
+    double idx;
 
-template <int DIR, int PREC>
-__global__ void __launch_bounds__(128) k_flux(Batch b)
+    __device__ static constexpr int perm(int q)
+    {
+        return DIR == 0 ? q : (q == 1 ? (DIR == 1 ? 2 : 3) : (q == (DIR == 1 ? 2 : 3) ? 1 : q));
+    }
+
+    __device__ __forceinline__ void state(int side, double W[5]) const
+    {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) W[q] = __ldg(f->rec[side * 5 + perm(q)] + c);
+    }
+
+    // DWxl = 2(Wl - WL)/dx, DWxr = 2(WR - Wr)/dx; transverse central differences of
+    // the neighbouring lines' states (update.cpp:253-260, 327-334, 416-423)
+    __device__ __forceinline__ void slopes(int side, S DW[3][5]) const
+    {
+        const double ys = DIR == 1 ? -0.5 : 0.5;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double *r = f->rec[side * 5 + perm(q)];
+            const double w = __ldg(r + c);
+            const double cell = __ldg(f->W[perm(q)] + (side == 0 ? c : c1));
+            DW[0][q] = S(2.0 * (side == 0 ? w - cell : cell - w) * idx);
+            DW[1][q] = S(ys * (__ldg(r + cn) - __ldg(r + cs)) * idx);
+            DW[2][q] = S(0.5 * (__ldg(r + cf) - __ldg(r + cb)) * idx);
+        }
+    }
+
+    __device__ __forceinline__ void cells(double WL[5], double WR[5]) const
+    {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            WL[q] = __ldg(f->W[perm(q)] + c);
+            WR[q] = __ldg(f->W[perm(q)] + c1);
+        }
+    }
+};
+
+template <int DIR, int PREC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_flux(Batch b)
 {
     using S = typename std::conditional<PREC == 0, double, float>::type;
-    constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
-    const double ysign = DIR == 1 ? -0.5 : 0.5;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
         const Cell x = decode(it - f.base, f.nc);
-        const long long c = x.c, c1 = along<DIR>(x, 1);
-        long long cn, cs, cf, cb;
-        transverse<DIR>(x, f.flags, cn, cs, cf, cb);
-        const double idx = f.inv_dx;
-
-        double WL[5], WR[5], Wl[5], Wr[5];
-        S DWl[3][5], DWr[3][5];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            WL[q] = __ldg(f.W[q] + c);
-            WR[q] = __ldg(f.W[q] + c1);
-            Wl[q] = __ldg(f.rec[q] + c);
-            Wr[q] = __ldg(f.rec[5 + q] + c);
-            DWl[0][q] = S(2.0 * (Wl[q] - WL[q]) * idx);
-            DWr[0][q] = S(2.0 * (WR[q] - Wr[q]) * idx);
-            DWl[1][q] = S(ysign * (__ldg(f.rec[q] + cn) - __ldg(f.rec[q] + cs)) * idx);
-            DWr[1][q] = S(ysign * (__ldg(f.rec[5 + q] + cn) - __ldg(f.rec[5 + q] + cs)) * idx);
-            DWl[2][q] = S(0.5 * (__ldg(f.rec[q] + cf) - __ldg(f.rec[q] + cb)) * idx);
-            DWr[2][q] = S(0.5 * (__ldg(f.rec[5 + q] + cf) - __ldg(f.rec[5 + q] + cb)) * idx);
-        }
-        // collision time at the left cell, before rotation (update.cpp:262-264)
+        SweepSrc<DIR, S> src;
+        src.f = &f;
+        src.c = x.c;
+        src.c1 = along<DIR>(x, 1);
+        transverse<DIR>(x, f.flags, src.cn, src.cs, src.cf, src.cb);
+        src.idx = f.inv_dx;
+        // collision time at the left cell, in the unrotated frame (update.cpp:262-264)
         double tau0;
         {
+            double WL[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) WL[q] = __ldg(f.W[q] + x.c);
             const double ri = __drcp_rn(WL[0]);
             const double P = f.gm1 * (WL[4] - 0.5 * (WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]) * ri);
             const double T = P * ri * (1.0 / f.R);
             tau0 = viscosity(f, T) * __drcp_rn(P);
-        }
-        if (ROT) {
-            rot5(WL, ROT); rot5(WR, ROT); rot5(Wl, ROT); rot5(Wr, ROT);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) { rot5(DWl[d], ROT); rot5(DWr[d], ROT); }
         }
         FluxConst fc;
         fc.gm1 = f.gm1;
@@ -237,10 +257,15 @@ __global__ void __launch_bounds__(128) k_flux(Batch b)
         fc.kA = f.kA;
         fc.K = f.K;
         double F[5];
-        gks_flux<S>(WL, WR, Wl, Wr, DWl, DWr, tau0, fc, F);
-        if (ROT) rot5(F, ROT);
+        gks_flux<S>(src, tau0, fc, F);
+        constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
+        if (ROT) {
+            const double t = F[1];
+            F[1] = F[ROT];
+            F[ROT] = t;
+        }
 #pragma unroll
-        for (int q = 0; q < 5; ++q) f.F[DIR * 5 + q][c] = F[q];
+        for (int q = 0; q < 5; ++q) f.F[DIR * 5 + q][x.c] = F[q];
     }
 }
 
@@ -532,40 +557,69 @@ int grid_for(long long items, int block)
     return int(g);
 }
 
-template <int PREC>
-cudaError_t recon_dispatch(const Batch &b, int dir, LaunchCfg cfg, cudaStream_t st)
-{
-    if (dir == 0) k_recon<0, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
-    else if (dir == 1) k_recon<1, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
-    else k_recon<2, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
-    return cudaGetLastError();
-}
-
-template <int PREC>
-cudaError_t flux_dispatch(const Batch &b, int dir, LaunchCfg cfg, cudaStream_t st)
-{
-    if (dir == 0) k_flux<0, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
-    else if (dir == 1) k_flux<1, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
-    else k_flux<2, PREC><<<cfg.grid, cfg.block, 0, st>>>(b);
-    return cudaGetLastError();
-}
-
 template <typename KernelT>
 cudaError_t occ(KernelT k, int block, int *n)
 {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k, block, 0);
 }
 
+// Register-cap variants (min resident blocks of 128 threads per SM); the
+// tuner picks one per kernel, precision and sweep.
+constexpr int kReconMinb[kReconVariants] = {4, 6};
+constexpr int kFluxMinb[kFluxVariants] = {1, 3, 4};
+
+template <int DIR, int PREC>
+cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
+{
+    switch (cfg.variant) {
+    case 1: k_recon<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    default: k_recon<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    }
+    return cudaGetLastError();
+}
+
+template <int DIR, int PREC>
+cudaError_t flux_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
+{
+    switch (cfg.variant) {
+    case 1: k_flux<DIR, PREC, kFluxMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    case 2: k_flux<DIR, PREC, kFluxMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    default: k_flux<DIR, PREC, kFluxMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    }
+    return cudaGetLastError();
+}
+
+template <int DIR, int PREC>
+cudaError_t occ_kind(int kind, int variant, int block, int *n)
+{
+    if (kind == K_RECON) {
+        if (variant == 1) return occ(k_recon<DIR, PREC, kReconMinb[1]>, block, n);
+        return occ(k_recon<DIR, PREC, kReconMinb[0]>, block, n);
+    }
+    if (variant == 1) return occ(k_flux<DIR, PREC, kFluxMinb[1]>, block, n);
+    if (variant == 2) return occ(k_flux<DIR, PREC, kFluxMinb[2]>, block, n);
+    return occ(k_flux<DIR, PREC, kFluxMinb[0]>, block, n);
+}
+
+template <int PREC>
+cudaError_t occ_dir(int kind, int dir, int variant, int block, int *n)
+{
+    return dir == 0 ? occ_kind<0, PREC>(kind, variant, block, n)
+                    : dir == 1 ? occ_kind<1, PREC>(kind, variant, block, n) : occ_kind<2, PREC>(kind, variant, block, n);
+}
+
 } // namespace
 
 cudaError_t launch_recon(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st)
 {
-    return prec == 0 ? recon_dispatch<0>(b, dir, cfg, st) : recon_dispatch<1>(b, dir, cfg, st);
+    if (prec == 0) return dir == 0 ? recon_go<0, 0>(b, cfg, st) : dir == 1 ? recon_go<1, 0>(b, cfg, st) : recon_go<2, 0>(b, cfg, st);
+    return dir == 0 ? recon_go<0, 1>(b, cfg, st) : dir == 1 ? recon_go<1, 1>(b, cfg, st) : recon_go<2, 1>(b, cfg, st);
 }
 
 cudaError_t launch_flux(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st)
 {
-    return prec == 0 ? flux_dispatch<0>(b, dir, cfg, st) : flux_dispatch<1>(b, dir, cfg, st);
+    if (prec == 0) return dir == 0 ? flux_go<0, 0>(b, cfg, st) : dir == 1 ? flux_go<1, 0>(b, cfg, st) : flux_go<2, 0>(b, cfg, st);
+    return dir == 0 ? flux_go<0, 1>(b, cfg, st) : dir == 1 ? flux_go<1, 1>(b, cfg, st) : flux_go<2, 1>(b, cfg, st);
 }
 
 cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st)
@@ -574,15 +628,10 @@ cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t max_resident_blocks(int kind, int dir, int prec, int block, int *n)
+cudaError_t max_resident_blocks(int kind, int dir, int prec, int variant, int block, int *n)
 {
     if (kind == K_UPDATE) return occ(k_update, block, n);
-    if (kind == K_RECON) {
-        if (prec == 0) return dir == 0 ? occ(k_recon<0, 0>, block, n) : dir == 1 ? occ(k_recon<1, 0>, block, n) : occ(k_recon<2, 0>, block, n);
-        return dir == 0 ? occ(k_recon<0, 1>, block, n) : dir == 1 ? occ(k_recon<1, 1>, block, n) : occ(k_recon<2, 1>, block, n);
-    }
-    if (prec == 0) return dir == 0 ? occ(k_flux<0, 0>, block, n) : dir == 1 ? occ(k_flux<1, 0>, block, n) : occ(k_flux<2, 0>, block, n);
-    return dir == 0 ? occ(k_flux<0, 1>, block, n) : dir == 1 ? occ(k_flux<1, 1>, block, n) : occ(k_flux<2, 1>, block, n);
+    return prec == 0 ? occ_dir<0>(kind, dir, variant, block, n) : occ_dir<1>(kind, dir, variant, block, n);
 }
 
 cudaError_t launch_gather(const FieldDev &f, const double *stage, cudaStream_t st)

@@ -40,21 +40,25 @@ struct Batch {
     int *err;         // device error word (bit 0: non-finite / non-positive state after update)
 };
 
-// Launch configuration chosen by the tuner per kernel kind.
+// Launch configuration chosen by the tuner per kernel kind and sweep: block
+// size, persistent grid, and the register-cap variant of the kernel.
 struct LaunchCfg {
     int block;
     int grid;
+    int variant;
 };
 
 enum KernelKind { K_RECON = 0, K_FLUX = 1, K_UPDATE = 2, K_KINDS = 3 };
+constexpr int kReconVariants = 2;
+constexpr int kFluxVariants = 3;
 
 // Stage launchers (asynchronous on `st`).  prec: 0 FP64, 1 mixed.
 cudaError_t launch_recon(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);
 cudaError_t launch_flux(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);
 cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st);
 
-// Occupancy-based persistent grid for a kernel kind.
-cudaError_t max_resident_blocks(int kind, int dir, int prec, int block, int *blocks_per_sm);
+// Resident blocks per SM of a kernel kind / variant (for persistent grids).
+cudaError_t max_resident_blocks(int kind, int dir, int prec, int variant, int block, int *blocks_per_sm);
 
 // Layout conversion of one field: padded host layout (5 x nt^3, contiguous) <-> interior.
 cudaError_t launch_gather(const FieldDev &f, const double *stage, cudaStream_t st);

@@ -1,0 +1,88 @@
+// Drop-in for the reference's GPU call site.
+//
+// The reference's WENO driver calls, once per step,
+//     void evolve(ptype *W[5], DevAlloc *dev, ptype dt);      weno/src/GPUupdate.h:33
+// with a DevAlloc created once at the start of Evolve (update.cpp:58) and the
+// grid / physics constants read from the globals of param.h.  This header
+// provides the same two names on top of the gks_b200 C ABI: include it in
+// place of "GPUupdate.h" and "GPUAlloc.h" (update.h:32-33), compile with
+// -DUseGPU and link -lgks_b200.  The call site in update.cpp stays unchanged.
+//
+// Semantics: one periodic block per process (procDim 1x1x1; the kernels wrap
+// the halo themselves, so a multi-rank decomposition is refused), FP64 by
+// default.  Compile-time options:
+//   GKS_COMPAT_MIXED          use the mixed FP32/FP64 path
+//   GKS_COMPAT_GPU_SEMANTICS  reproduce the reference GPU kernel's choices
+//                             (WENO on rho E, no 1/Pr factor) instead of the
+//                             CPU path's (the parity default)
+// As in the reference, evolve() uploads W, advances one step and downloads W;
+// the downloaded ghosts already hold the periodic image, so the caller's
+// HaloTransfer that follows leaves them unchanged.
+#pragma once
+
+#include <cstdio>
+#include <cstdlib>
+
+#include "gks_b200.h"
+
+static_assert(sizeof(ptype) == sizeof(double), "gks_b200 advances double-precision fields");
+
+class DevAlloc
+{
+public:
+    DevAlloc();
+    ~DevAlloc() { gks_destroy(ctx); }
+    DevAlloc(const DevAlloc &) = delete;
+    DevAlloc &operator=(const DevAlloc &) = delete;
+    gks_ctx *ctx = nullptr;
+};
+
+inline void gks_compat_check(gks_ctx *ctx, int rc, const char *what)
+{
+    if (rc == GKS_OK) return;
+    fprintf(stderr, "gks_b200: %s failed (%d): %s\n", what, rc, gks_last_error(ctx));
+    abort(); // the reference signature has no error return
+}
+
+inline DevAlloc::DevAlloc()
+{
+    if (procDim[0] * procDim[1] * procDim[2] != 1 || nc_segx != nc_segy || nc_segx != nc_segz) {
+        fprintf(stderr, "gks_b200: one periodic cube per process is required (procDim 1x1x1)\n");
+        abort();
+    }
+    gks_phys p{};
+    p.nc = nc_segx;
+    p.K = K;
+    p.visc_law = GKS_VISC_SUTHERLAND; // update.cpp:263
+    p.gam = gam;
+    p.gas_r = R;
+    p.T0 = T0;
+    p.mu0 = mu0;
+    p.visc_exp = 0.76;
+#ifdef GKS_COMPAT_GPU_SEMANTICS
+    p.pr_factor = 1.0; // GPUupdate.cu:839
+    const int flags = GKS_DIRECT_ENERGY;
+#else
+    p.pr_factor = 1 / 0.7; // GKMflux.cpp:289
+    const int flags = 0;
+#endif
+    p.p0 = p0;
+    p.den0 = den0;
+    p.Mt = Mt;
+    p.t0 = t0;
+#ifdef GKS_COMPAT_MIXED
+    const int precision = GKS_MIXED;
+#else
+    const int precision = GKS_FP64;
+#endif
+    gks_compat_check(nullptr, gks_create(&ctx, 1, &p, precision, flags), "gks_create");
+}
+
+inline void evolve(ptype *W[5], DevAlloc *dev, ptype dt)
+{
+    gks_compat_check(dev->ctx, gks_upload(dev->ctx, 0, W), "gks_upload");
+    gks_compat_check(dev->ctx, gks_set_dt(dev->ctx, 0, dt), "gks_set_dt");
+    gks_compat_check(dev->ctx, gks_step(dev->ctx, 1), "gks_step");
+    gks_compat_check(dev->ctx, gks_sync(dev->ctx), "gks_sync");
+    gks_compat_check(dev->ctx, gks_download(dev->ctx, 0, W), "gks_download");
+}

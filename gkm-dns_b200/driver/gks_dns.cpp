@@ -122,7 +122,7 @@ int main(int argc, char **argv)
     ph.K = p.K();
     ph.visc_law = o.visc_law;
     ph.gam = p.gam;
-    ph.R = p.R;
+    ph.gas_r = p.R;
     ph.T0 = p.T0();
     ph.mu0 = p.mu0;
     ph.visc_exp = o.visc_exp;

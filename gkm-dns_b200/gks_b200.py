@@ -44,7 +44,7 @@ class GksError(RuntimeError):
 class Phys(ctypes.Structure):
     _fields_ = [
         ("nc", ctypes.c_int), ("K", ctypes.c_int), ("visc_law", ctypes.c_int), ("reserved", ctypes.c_int),
-        ("gam", ctypes.c_double), ("R", ctypes.c_double), ("T0", ctypes.c_double), ("mu0", ctypes.c_double),
+        ("gam", ctypes.c_double), ("gas_r", ctypes.c_double), ("T0", ctypes.c_double), ("mu0", ctypes.c_double),
         ("visc_exp", ctypes.c_double), ("pr_factor", ctypes.c_double),
         ("p0", ctypes.c_double), ("den0", ctypes.c_double), ("Mt", ctypes.c_double), ("t0", ctypes.c_double),
     ]
@@ -86,6 +86,9 @@ SIGNATURES = {
     "gks_select_device": (ctypes.c_int, [ctypes.c_int]),
     "gks_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP]),
     "gks_peak_flops": (ctypes.c_int, [ctypes.c_int, DP]),
+    "gks_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "gks_get_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
 }
 
 STAGES = ["recon_x", "flux_x", "recon_y", "flux_y", "recon_z", "flux_z", "update"]
@@ -126,7 +129,7 @@ def load_library(path: str = LIB_PATH):
 
 def phys_from_case(case, visc_law=VISC_SUTHERLAND, visc_exp=0.76, pr_factor=PR_FACTOR_CPU) -> Phys:
     """gks_phys from a gks_ic.DhitCase (or any object with its attributes)."""
-    return Phys(nc=case.nc, K=case.K, visc_law=visc_law, reserved=0, gam=case.gam, R=287.0, T0=case.T0,
+    return Phys(nc=case.nc, K=case.K, visc_law=visc_law, reserved=0, gam=case.gam, gas_r=287.0, T0=case.T0,
                 mu0=case.mu0, visc_exp=visc_exp, pr_factor=pr_factor, p0=case.p0, den0=case.rho0, Mt=case.Mt,
                 t0=case.t0)
 
@@ -241,6 +244,19 @@ class Solver:
         ms = (ctypes.c_double * 7)()
         self._ck(self._lib.gks_time_stages(self._h, reps, ms))
         return dict(zip(STAGES, list(ms)))
+
+    def autotune(self, reps: int = 2):
+        """Pick register-cap variant and grid of every reconstruction / flux kernel."""
+        self._ck(self._lib.gks_autotune(self._h, reps))
+
+    def launch_config(self) -> dict:
+        out = {}
+        for kind, kname in enumerate(("recon", "flux", "update")):
+            for d, dname in enumerate("xyz"):
+                b, g, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+                self._ck(self._lib.gks_get_launch(self._h, kind, d, ctypes.byref(b), ctypes.byref(g), ctypes.byref(v)))
+                out[f"{kname}_{dname}"] = {"block": b.value, "grid": g.value, "variant": v.value}
+        return out
 
     def set_stream(self, stream: int | None):
         self._ck(self._lib.gks_set_stream(self._h, ctypes.c_void_p(stream or 0)))

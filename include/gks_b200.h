@@ -70,7 +70,7 @@ typedef struct {
     int visc_law;     /* GKS_VISC_* */
     int reserved;
     double gam;       /* ratio of specific heats */
-    double R;         /* gas constant (287, param.h:18) */
+    double gas_r;     /* gas constant R (287, param.h:18); not named R, which param.h defines as a macro */
     double T0;        /* p0 / (R rho0) (FlowField.cpp:46) */
     double mu0;       /* viscosity at T0 */
     double visc_exp;  /* exponent of GKS_VISC_POWER */
@@ -145,6 +145,17 @@ int gks_select_device(int device);
  * between them; ms[0..6] receives the mean time of recon x, flux x, recon y,
  * flux y, recon z, flux z, update.  For profiling: the state advances. */
 int gks_time_stages(gks_ctx *ctx, int reps, double *ms);
+
+/* Tune the launch configuration of the reconstruction and flux kernels of
+ * every sweep on the context's current fields: register-cap variant (resident
+ * blocks per SM) and persistent grid size, each candidate timed with CUDA
+ * events over `reps` launches.  Results are cached per process by device,
+ * precision, flags and field sizes; the state is not modified. */
+int gks_autotune(gks_ctx *ctx, int reps);
+
+/* The launch configuration in use: kind 0 reconstruction, 1 flux, 2 update;
+ * dir 0..2 = x, y, z. */
+int gks_get_launch(gks_ctx *ctx, int kind, int dir, int *block, int *grid, int *variant);
 
 /* Peak FMA throughput of the FP64 (GKS_FP64) or FP32 (GKS_MIXED) pipe of
  * the current device in TFLOP/s, 2 flops per FMA (a short microbenchmark). */

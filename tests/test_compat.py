@@ -1,0 +1,85 @@
+"""The reference call-site shim (gkm-dns_b200/driver/gks_compat.h) and the
+drop-in driver (gks_dns) against the reference's file formats."""
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG, ROOT
+
+import gks_ic
+
+COMPAT_SRC = os.path.join(ROOT, "tests", "compat", "compat_main.cpp")
+
+
+def build_compat(out):
+    cmd = ["g++", "-O2", "-std=c++17", f"-I{ROOT}/include", f"-I{PKG}/driver", COMPAT_SRC, "-o", out,
+           f"-L{PKG}/lib", "-lgks_b200", f"-Wl,-rpath,{PKG}/lib"]
+    subprocess.run(cmd, check=True)
+
+
+def test_compat_header_compiles(tmp_path):
+    build_compat(str(tmp_path / "compat_main"))
+
+
+def test_driver_rejects_missing_case(tmp_path):
+    exe = os.path.join(PKG, "driver", "gks_dns")
+    assert os.path.exists(exe)
+    r = subprocess.run([exe, "--case", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 2 and "cannot open" in r.stderr
+
+
+def test_driver_rejects_short_init(tmp_path):
+    case = gks_ic.make_dhit(8, seed=0)
+    gks_ic.write_case(str(tmp_path), case)
+    p = tmp_path / "InitialConditions" / "Init000"
+    p.write_bytes(p.read_bytes()[:1000])
+    r = subprocess.run([os.path.join(PKG, "driver", "gks_dns"), "--case", str(tmp_path)], capture_output=True,
+                       text=True)
+    assert r.returncode == 2 and "shorter" in r.stderr
+
+
+@pytest.mark.gpu
+def test_compat_evolve_matches_solver(tmp_path, gks):
+    case = gks_ic.make_dhit(16, k0=4.0, Mt=0.3, seed=5)
+    W = gks_ic.to_conservative_padded(case)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W)
+        dt = s.timestep(0.5)
+        s.step(3)
+        s.sync()
+        ref = s.download()
+    exe = str(tmp_path / "compat_main")
+    build_compat(exe)
+    W.tofile(str(tmp_path / "in.bin"))
+    subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), "16", repr(dt), "3", repr(case.gam),
+                    repr(case.mu0), repr(case.p0), "1.0", repr(case.Mt), repr(case.t0)], check=True)
+    got = np.fromfile(str(tmp_path / "out.bin")).reshape(W.shape)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.gpu
+def test_driver_prints_reference_lines(tmp_path, oracle):
+    """gks_dns on the 16^3 golden case prints the reference's statistics lines."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "dhit16.npz"))
+    case = gks_ic.make_dhit(16, seed=1)
+    gks_ic.write_case(str(tmp_path), case)
+    r = subprocess.run([os.path.join(PKG, "driver", "gks_dns"), "--case", str(tmp_path), "--cfl", "0.5",
+                        "--steps", "10", "--reinit", str(tmp_path / "final")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip() and ln.strip()[0].isdigit()]
+    ref = [str(x) for x in g["lines"]]
+    assert len(lines) == 11 and len(ref) == 11
+    for a, b in zip(lines, ref):
+        va = [float(x) for x in a.split()]
+        vb = [float(x) for x in b.split()]
+        np.testing.assert_allclose(va, vb, rtol=2e-8, atol=1e-12)
+        assert a.count("  ") == b.count("  ")
+    # the reinit file holds the final state in the Init layout
+    raw = np.fromfile(str(tmp_path / "final"))
+    assert raw.size == 5 * 16**3
+    u = raw[:16**3].reshape(16, 16, 16).transpose(2, 1, 0)
+    w10 = g["w10"]
+    np.testing.assert_allclose(u, w10[1] / w10[0], rtol=0, atol=1e-12)

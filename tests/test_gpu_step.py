@@ -217,6 +217,25 @@ def test_ensemble_equals_individual_runs(gks):
                 assert np.array_equal(s.download(f), alone[f])
 
 
+def test_autotuned_launches_give_identical_results(gks):
+    case = gks_ic.make_dhit(24, k0=4.0, Mt=0.5, seed=8)
+    W = gks_ic.to_conservative_padded(case)
+    for prec in (gks.FP64, gks.MIXED):
+        out = []
+        for tune in (False, True):
+            with gks.Solver(gks.phys_from_case(case), prec) as s:
+                s.upload(W)
+                s.timestep(0.5)
+                if tune:
+                    s.autotune(1)
+                    cfg = s.launch_config()
+                    assert all(v["grid"] >= 1 for v in cfg.values())
+                s.step(3)
+                s.sync()
+                out.append(s.download())
+        assert np.array_equal(out[0], out[1])
+
+
 def test_mixed_tracks_fp64(gks):
     case = gks_ic.make_dhit(32, k0=4.0, Mt=0.5, Re_lambda=100.0, seed=0)
     W = gks_ic.to_conservative_padded(case)
