@@ -224,7 +224,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     if (flags & ~(GKS_FIX_ZSWEEP | GKS_DIRECT_ENERGY)) return GKS_EINVAL;
     for (int f = 0; f < nfields; ++f) {
         const gks_phys &p = phys[f];
-        if (p.nc < 4 || p.nc > 4096 || !(p.gam > 1.0) || !(p.gas_r > 0) || !(p.T0 > 0) || !(p.mu0 >= 0) ||
+        if (p.nc < 4 || p.nc > 1024 || !(p.gam > 1.0) || !(p.gas_r > 0) || !(p.T0 > 0) || !(p.mu0 >= 0) ||
             p.K < 0 || (p.visc_law != GKS_VISC_SUTHERLAND && p.visc_law != GKS_VISC_POWER) || !(p.pr_factor > 0))
             return GKS_EINVAL;
     }
@@ -268,8 +268,16 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.spl_inv = h.spl + nt;
         d.base = base;
         d.ncell = n;
-        base += n;
+        base += (n + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
         d.nc = p.nc;
+        // magic number for x / nc (round-up method): l = ceil(log2 nc),
+        // m = floor(2^32 (2^l - nc) / nc) + 1, x / nc = (umulhi(x, m) + x) >> l
+        {
+            int l = 0;
+            while ((1u << l) < (unsigned)p.nc) ++l;
+            d.nc_shift = l;
+            d.nc_magic = (unsigned)(((1ull << 32) * ((1ull << l) - (unsigned)p.nc)) / (unsigned)p.nc + 1);
+        }
         d.K = p.K;
         d.visc_law = p.visc_law;
         d.flags = flags;

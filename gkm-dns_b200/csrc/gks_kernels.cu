@@ -32,33 +32,40 @@ __device__ __forceinline__ int field_of(const FieldDev *f, int n, long long it)
 
 struct Cell {
     int j, i, k, nc;
-    long long c;
+    unsigned c; // (j*nc + i)*nc + k
 };
 
-__device__ __forceinline__ Cell decode(long long c, int nc)
+// x / nc by multiply-high with the field's precomputed magic number.
+__device__ __forceinline__ unsigned div_nc(unsigned x, const FieldDev &f)
+{
+    return (unsigned)(((unsigned long long)__umulhi(x, f.nc_magic) + x) >> f.nc_shift);
+}
+
+__device__ __forceinline__ Cell decode(unsigned c, const FieldDev &f)
 {
     Cell x;
-    x.nc = nc;
+    x.nc = f.nc;
     x.c = c;
-    x.k = int(c % nc);
-    const long long r = c / nc;
-    x.i = int(r % nc);
-    x.j = int(r / nc);
+    const unsigned r = div_nc(c, f);
+    x.k = int(c - r * f.nc);
+    const unsigned jj = div_nc(r, f);
+    x.i = int(r - jj * f.nc);
+    x.j = int(jj);
     return x;
 }
 
 __device__ __forceinline__ int wrap(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 
 // Linear index of the cell displaced by (dj, di, dk), periodic.
-__device__ __forceinline__ long long shift(const Cell &x, int dj, int di, int dk)
+__device__ __forceinline__ unsigned shift(const Cell &x, int dj, int di, int dk)
 {
-    const int n = x.nc;
-    return ((long long)wrap(x.j + dj, n) * n + wrap(x.i + di, n)) * n + wrap(x.k + dk, n);
+    const unsigned n = x.nc;
+    return ((unsigned)wrap(x.j + dj, x.nc) * n + (unsigned)wrap(x.i + di, x.nc)) * n + (unsigned)wrap(x.k + dk, x.nc);
 }
 
 // Displacement along the sweep axis: DIR 0 = x (i), 1 = y (j), 2 = z (k).
 template <int DIR>
-__device__ __forceinline__ long long along(const Cell &x, int d)
+__device__ __forceinline__ unsigned along(const Cell &x, int d)
 {
     return DIR == 0 ? shift(x, 0, d, 0) : (DIR == 1 ? shift(x, d, 0, 0) : shift(x, 0, 0, d));
 }
@@ -88,8 +95,9 @@ __global__ void __launch_bounds__(128, MINB) k_recon(Batch b)
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
-        const Cell x = decode(it - f.base, f.nc);
-        long long idx[6];
+        if (it - f.base >= f.ncell) continue; // alignment padding after the field
+        const Cell x = decode(unsigned(it - f.base), f);
+        unsigned idx[6];
 #pragma unroll
         for (int a = 0; a < 6; ++a) idx[a] = along<DIR>(x, a - 2);
         double s[6][5];
@@ -159,8 +167,8 @@ __global__ void __launch_bounds__(128, MINB) k_recon(Batch b)
 // Momentum is rotated into slot 1 for y (rho v) and z (rho w).
 // ---------------------------------------------------------------------------
 template <int DIR>
-__device__ __forceinline__ void transverse(const Cell &x, int flags, long long &n, long long &s,
-                                           long long &fr, long long &bk)
+__device__ __forceinline__ void transverse(const Cell &x, int flags, unsigned &n, unsigned &s, unsigned &fr,
+                                           unsigned &bk)
 {
     if (DIR == 0) {
         n = shift(x, 1, 0, 0); s = shift(x, -1, 0, 0);
@@ -179,74 +187,105 @@ __device__ __forceinline__ void transverse(const Cell &x, int flags, long long &
     }
 }
 
-// Inputs of one interface, read on demand (see gks_flux).  Slot q of the
-// rotated frame holds original component perm(q): rho v (y sweep) or rho w
-// (z sweep) moves into slot 1 (update.cpp:340-350, 429-439).
+// Inputs of one interface (see gks_flux).  All global loads are issued at
+// once when the interface starts, so that their latency overlaps; what is not
+// needed until later -- the right state's slopes and the two cell averages --
+// is parked in this thread's own shared-memory slots ([slot][thread], no bank
+// conflicts) instead of registers.  Slot q of the rotated frame holds
+// original component perm(q): rho v (y sweep) or rho w (z sweep) moves into
+// slot 1 (update.cpp:340-350, 429-439).
+constexpr int kFluxBlock = 128;
+
 template <int DIR, typename S>
 struct SweepSrc {
-    const FieldDev *f;
-    long long c, c1, cn, cs, cf, cb;
-    double idx;
+    double Wl[5], Wr[5];
+    S DWl[3][5];
+    S (*park_dw)[kFluxBlock];      // [15][block]: right-side slopes
+    double (*park_w)[kFluxBlock];  // [10][block]: WL, WR
 
     __device__ static constexpr int perm(int q)
     {
         return DIR == 0 ? q : (q == 1 ? (DIR == 1 ? 2 : 3) : (q == (DIR == 1 ? 2 : 3) ? 1 : q));
     }
 
+    // DWxl = 2(Wl - WL)/dx, DWxr = 2(WR - Wr)/dx; transverse central differences of
+    // the neighbouring lines' states (update.cpp:253-260, 327-334, 416-423)
+    __device__ __forceinline__ void load(const FieldDev &f, unsigned c, unsigned c1, unsigned cn, unsigned cs,
+                                         unsigned cf, unsigned cb)
+    {
+        const double idx = f.inv_dx, ys = DIR == 1 ? -0.5 : 0.5;
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const int o = perm(q);
+            const double *rl = f.rec[o], *rr = f.rec[5 + o];
+            const double wL = __ldg(f.W[o] + c), wR = __ldg(f.W[o] + c1);
+            Wl[q] = __ldg(rl + c);
+            Wr[q] = __ldg(rr + c);
+            DWl[0][q] = S(2.0 * (Wl[q] - wL) * idx);
+            DWl[1][q] = S(ys * (__ldg(rl + cn) - __ldg(rl + cs)) * idx);
+            DWl[2][q] = S(0.5 * (__ldg(rl + cf) - __ldg(rl + cb)) * idx);
+            park_dw[q][t] = S(2.0 * (wR - Wr[q]) * idx);
+            park_dw[5 + q][t] = S(ys * (__ldg(rr + cn) - __ldg(rr + cs)) * idx);
+            park_dw[10 + q][t] = S(0.5 * (__ldg(rr + cf) - __ldg(rr + cb)) * idx);
+            park_w[q][t] = wL;
+            park_w[5 + q][t] = wR;
+        }
+    }
+
     __device__ __forceinline__ void state(int side, double W[5]) const
     {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) W[q] = __ldg(f->rec[side * 5 + perm(q)] + c);
+        for (int q = 0; q < 5; ++q) W[q] = side == 0 ? Wl[q] : Wr[q];
     }
 
-    // DWxl = 2(Wl - WL)/dx, DWxr = 2(WR - Wr)/dx; transverse central differences of
-    // the neighbouring lines' states (update.cpp:253-260, 327-334, 416-423)
     __device__ __forceinline__ void slopes(int side, S DW[3][5]) const
     {
-        const double ys = DIR == 1 ? -0.5 : 0.5;
+        const int t = threadIdx.x;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            const double *r = f->rec[side * 5 + perm(q)];
-            const double w = __ldg(r + c);
-            const double cell = __ldg(f->W[perm(q)] + (side == 0 ? c : c1));
-            DW[0][q] = S(2.0 * (side == 0 ? w - cell : cell - w) * idx);
-            DW[1][q] = S(ys * (__ldg(r + cn) - __ldg(r + cs)) * idx);
-            DW[2][q] = S(0.5 * (__ldg(r + cf) - __ldg(r + cb)) * idx);
-        }
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) DW[d][q] = side == 0 ? DWl[d][q] : park_dw[5 * d + q][t];
     }
 
     __device__ __forceinline__ void cells(double WL[5], double WR[5]) const
     {
+        const int t = threadIdx.x;
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            WL[q] = __ldg(f->W[perm(q)] + c);
-            WR[q] = __ldg(f->W[perm(q)] + c1);
+            WL[q] = park_w[q][t];
+            WR[q] = park_w[5 + q][t];
         }
     }
 };
 
 template <int DIR, int PREC, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_flux(Batch b)
+__global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
 {
     using S = typename std::conditional<PREC == 0, double, float>::type;
+    __shared__ S park_dw[15][kFluxBlock];
+    __shared__ double park_w[10][kFluxBlock];
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
-        const Cell x = decode(it - f.base, f.nc);
+        if (it - f.base >= f.ncell) continue; // alignment padding after the field
+        const Cell x = decode(unsigned(it - f.base), f);
+        unsigned cn, cs, cf, cb;
+        transverse<DIR>(x, f.flags, cn, cs, cf, cb);
         SweepSrc<DIR, S> src;
-        src.f = &f;
-        src.c = x.c;
-        src.c1 = along<DIR>(x, 1);
-        transverse<DIR>(x, f.flags, src.cn, src.cs, src.cf, src.cb);
-        src.idx = f.inv_dx;
+        src.park_dw = park_dw;
+        src.park_w = park_w;
+        src.load(f, x.c, along<DIR>(x, 1), cn, cs, cf, cb);
         // collision time at the left cell, in the unrotated frame (update.cpp:262-264)
         double tau0;
         {
-            double WL[5];
+            double WL[5], WR[5];
+            src.cells(WL, WR);
+            double w[5];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) WL[q] = __ldg(f.W[q] + x.c);
-            const double ri = __drcp_rn(WL[0]);
-            const double P = f.gm1 * (WL[4] - 0.5 * (WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]) * ri);
+            for (int q = 0; q < 5; ++q) w[SweepSrc<DIR, S>::perm(q)] = WL[q];
+            const double ri = __drcp_rn(w[0]);
+            const double P = f.gm1 * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) * ri);
             const double T = P * ri * (1.0 / f.R);
             tau0 = viscosity(f, T) * __drcp_rn(P);
         }
@@ -279,9 +318,10 @@ __global__ void __launch_bounds__(256) k_update(Batch b)
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
-        const Cell x = decode(it - f.base, f.nc);
-        const long long c = x.c;
-        const long long cx = shift(x, 0, -1, 0), cy = shift(x, -1, 0, 0), cz = shift(x, 0, 0, -1);
+        if (it - f.base >= f.ncell) continue; // alignment padding after the field
+        const Cell x = decode(unsigned(it - f.base), f);
+        const unsigned c = x.c;
+        const unsigned cx = shift(x, 0, -1, 0), cy = shift(x, -1, 0, 0), cz = shift(x, 0, 0, -1);
         double w[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -308,7 +348,7 @@ __global__ void k_gather(FieldDev f, const double *__restrict__ stage)
     const long long Nt = (long long)nt * nt * nt;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
-        const Cell x = decode(c, nc);
+        const Cell x = decode(unsigned(c), f);
         const long long p = ((long long)(x.j + 3) * nt + (x.i + 3)) * nt + (x.k + 3);
 #pragma unroll
         for (int q = 0; q < 5; ++q) f.W[q][c] = stage[q * Nt + p];

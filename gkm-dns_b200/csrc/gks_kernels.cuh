@@ -20,9 +20,11 @@ struct FieldDev {
     double *F[15];    // Fx[0..4], Fy[0..4], Fz[0..4]
     const double *spl_cp;   // natural-spline Thomas coefficients, nt entries
     const double *spl_inv;  // reciprocal pivots, nt entries
-    long long base;   // first work item (cell) of this field in the batch
-    long long ncell;  // nc^3
+    long long base;   // first work item of this field in the batch (a multiple of kItemAlign)
+    long long ncell;  // nc^3 (< 2^31)
     int nc;
+    unsigned nc_magic; // x / nc == (umulhi(x, nc_magic) + x) >> nc_shift for 32-bit x
+    int nc_shift;
     int K;
     int visc_law;     // 0 Sutherland, 1 power law
     int flags;        // GKS_FIX_ZSWEEP | GKS_DIRECT_ENERGY
@@ -33,10 +35,14 @@ struct FieldDev {
     double spl_s;     // 3/h of the spline grid
 };
 
+// Field item ranges start at multiples of this, so that a block of up to
+// kItemAlign consecutive items never spans two fields.
+constexpr int kItemAlign = 256;
+
 struct Batch {
     FieldDev *fields; // device array
     int nfields;
-    long long total;  // sum of ncell
+    long long total;  // end of the last field's item range
     int *err;         // device error word (bit 0: non-finite / non-positive state after update)
 };
 

@@ -75,7 +75,9 @@ def test_driver_prints_reference_lines(tmp_path, oracle):
     for a, b in zip(lines, ref):
         va = [float(x) for x in a.split()]
         vb = [float(x) for x in b.split()]
-        np.testing.assert_allclose(va, vb, rtol=2e-8, atol=1e-12)
+        # columns 9-11 (p, T, 1/rho rms, O(0.1) once the flow develops) are pure
+        # round-off at t = 0, where pressure and density are uniform
+        np.testing.assert_allclose(va, vb, rtol=2e-8, atol=1e-10)
         assert a.count("  ") == b.count("  ")
     # the reinit file holds the final state in the Init layout
     raw = np.fromfile(str(tmp_path / "final"))
