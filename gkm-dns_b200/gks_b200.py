@@ -89,6 +89,8 @@ SIGNATURES = {
     "gks_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "gks_get_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "gks_timestep_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_void_p, DP]),
 }
 
 STAGES = ["recon_x", "flux_x", "recon_y", "flux_y", "recon_z", "flux_z", "update"]

@@ -161,6 +161,24 @@ int gks_get_launch(gks_ctx *ctx, int kind, int dir, int *block, int *grid, int *
  * the current device in TFLOP/s, 2 flops per FMA (a short microbenchmark). */
 int gks_peak_flops(int precision, double *tflops);
 
+/* The time step without allocating anything -- for callers that may not
+ * allocate device memory: host codes that own and pool every byte of device
+ * memory themselves, and loops that cannot afford cudaMalloc's implicit
+ * device synchronisation (gks_create, which gks_timestep needs, allocates).
+ * No counterpart in the reference: its timestep() (update.cpp:1057-1079) runs
+ * on the host.
+ * dW: the caller's five device arrays in this library's interior layout
+ * (nc^3 doubles each, index (j*nc + i)*nc + k), e.g. from gks_device_fields.
+ * Returns dt = cfl * (2 pi/nc) / max(|u| + c) in *dt_out (host memory), the
+ * same value gks_timestep gives, after synchronising `stream` (NULL: the
+ * legacy default stream).  Limit: nc <= 1024, else GKS_ETOOBIG.  Scratch is a
+ * fixed file-scope device array of 1026 64-bit words that every GPU loading
+ * the library holds until exit; the first call on a device looks up its
+ * address, so make that first call before any stream capture.  Calls share
+ * the scratch: calls that overlap on the GPU race and must be serialised. */
+int gks_timestep_noalloc(const double *const dW[5], int nc, double gam, double cfl, void *stream,
+                         double *dt_out);
+
 #ifdef __cplusplus
 }
 #endif
