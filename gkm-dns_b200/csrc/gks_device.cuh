@@ -35,6 +35,27 @@ template <typename T> __device__ __forceinline__ T rcp(T x);
 template <> __device__ __forceinline__ double rcp<double>(double x) { return __drcp_rn(x); }
 template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
 
+// Two FP32 lanes advanced by one paired instruction (f32x2 add/mul/fma of
+// sm_100): the mixed flux runs two structurally identical moment evaluations
+// (left and right Maxwellian, or two mirror-image equilibrium terms) as the
+// .x and .y lanes of one instruction stream.
+struct f2 {
+    float2 v;
+    f2() = default;
+    __device__ __forceinline__ f2(float s) : v(make_float2(s, s)) {}
+    __device__ __forceinline__ f2(float a, float b) : v(make_float2(a, b)) {}
+};
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) { f2 r; r.v = __fadd2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) { f2 r; r.v = __fmul2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { f2 r; r.v = __ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v); return r; }
+__device__ __forceinline__ f2 operator-(f2 a) { f2 r; r.v = __fmul2_rn(a.v, make_float2(-1.f, -1.f)); return r; }
+__device__ __forceinline__ f2 &operator+=(f2 &a, f2 b) { a = a + b; return a; }
+
+// a*b + c with one rounding, for every arithmetic type used here.
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ f2 fmaT(f2 a, f2 b, f2 c) { f2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r; }
+
 // ---------------------------------------------------------------------------
 // WENO-SYMOO on one scalar 6-point stencil (update.cpp:505-557): four cubic
 // candidates per side, linear weights 1/20, 9/20, 9/20, 1/20, the fourth
@@ -42,25 +63,26 @@ template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp
 // The normalised weights are formed with one reciprocal per side:
 // w_r = g_r prod_{s!=r} d_s / sum_t g_t prod_{s!=t} d_s, d = eps + IS.
 // ---------------------------------------------------------------------------
+// One side seen from (a, b, c | d, e, f): candidates on {a,b,c}, {b,c,d},
+// {c,d,e}, {d,e,f}; q0..q3 are 13/12 of the squared second differences of
+// those stencils, which both sides share.
 template <typename T>
-__device__ __forceinline__ void weno_side(T a, T b, T c, T d, T e, T f, T eps, T &out)
+__device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1, T q2, T q3, T eps)
 {
-    // side seen from (a, b, c | d, e, f): candidates on {a,b,c},{b,c,d},{c,d,e},{d,e,f}
     const T third = T(1) / T(3), sixth = T(1) / T(6);
     const T p0 = third * a - (T(7) * sixth) * b + (T(11) * sixth) * c;
     const T p1 = -sixth * b + (T(5) * sixth) * c + third * d;
     const T p2 = third * c + (T(5) * sixth) * d - sixth * e;
     const T p3 = (T(11) * sixth) * d - (T(7) * sixth) * e + third * f;
-    const T k13 = T(13) / T(12);
-    T s, t;
-    s = a - T(2) * b + c; t = a - T(4) * b + T(3) * c;
-    const T is0 = k13 * s * s + T(0.25) * t * t;
-    s = b - T(2) * c + d; t = d - b;
-    const T is1 = k13 * s * s + T(0.25) * t * t;
-    s = c - T(2) * d + e; t = T(-3) * c + T(4) * d - e;
-    const T is2 = k13 * s * s + T(0.25) * t * t;
-    s = d - T(2) * e + f; t = T(-5) * d + T(8) * e - T(3) * f;
-    T is3 = k13 * s * s + T(0.25) * t * t;
+    T t;
+    t = a - T(4) * b + T(3) * c;
+    const T is0 = fmaT(T(0.25), t * t, q0);
+    t = d - b;
+    const T is1 = fmaT(T(0.25), t * t, q1);
+    t = T(-3) * c + T(4) * d - e;
+    const T is2 = fmaT(T(0.25), t * t, q2);
+    t = T(-5) * d + T(8) * e - T(3) * f;
+    T is3 = fmaT(T(0.25), t * t, q3);
     is3 = fmax(fmax(fmax(is0, is1), is2), is3);
     const T d0 = eps + is0, d1 = eps + is1, d2 = eps + is2, d3 = eps + is3;
     const T d01 = d0 * d1, d23 = d2 * d3;
@@ -69,7 +91,7 @@ __device__ __forceinline__ void weno_side(T a, T b, T c, T d, T e, T f, T eps, T
     const T n2 = T(0.45) * (d01 * d3);
     const T n3 = T(0.05) * (d01 * d2);
     const T inv = rcp<T>(n0 + n1 + n2 + n3);
-    out = (n0 * p0 + n1 * p1 + n2 * p2 + n3 * p3) * inv;
+    return (n0 * p0 + n1 * p1 + n2 * p2 + n3 * p3) * inv;
 }
 
 // Both interface values of the stencil (LLL, LL, L, R, RR, RRR): wl seen from
@@ -77,8 +99,14 @@ __device__ __forceinline__ void weno_side(T a, T b, T c, T d, T e, T f, T eps, T
 template <typename T>
 __device__ __forceinline__ void weno_pair(T LLL, T LL, T L, T R, T RR, T RRR, T eps, T &wl, T &wr)
 {
-    weno_side<T>(LLL, LL, L, R, RR, RRR, eps, wl);
-    weno_side<T>(RRR, RR, R, L, LL, LLL, eps, wr);
+    const T k13 = T(13) / T(12);
+    T s;
+    s = LLL - T(2) * LL + L;  const T q0 = k13 * s * s;
+    s = LL - T(2) * L + R;    const T q1 = k13 * s * s;
+    s = L - T(2) * R + RR;    const T q2 = k13 * s * s;
+    s = R - T(2) * RR + RRR;  const T q3 = k13 * s * s;
+    wl = weno_side<T>(LLL, LL, L, R, RR, RRR, q0, q1, q2, q3, eps);
+    wr = weno_side<T>(RRR, RR, R, L, LL, LLL, q3, q2, q1, q0, eps);
 }
 
 // ---------------------------------------------------------------------------
@@ -88,10 +116,10 @@ __device__ __forceinline__ void weno_pair(T LLL, T LL, T L, T R, T RR, T RRR, T 
 template <int N, typename T>
 __device__ __forceinline__ void full_table(T U, T s, T *f)
 {
-    f[0] = T(1);
+    f[0] = T(1.0f);
     f[1] = U;
 #pragma unroll
-    for (int n = 2; n < N; ++n) f[n] = U * f[n - 1] + T(n - 1) * s * f[n - 2];
+    for (int n = 2; n < N; ++n) f[n] = fmaT(U, f[n - 1], (T(float(n - 1)) * s) * f[n - 2]);
 }
 
 // Half-space moments over u > 0 (sign = +1) or u < 0 (sign = -1), seeded by
@@ -131,23 +159,24 @@ __device__ __forceinline__ void mcal0(T M[5], const T *X, const T *Y, const T *Z
     M[1] = X[k + 1] * yz;
     M[2] = X[k] * (Y[l + 1] * Z[m]);
     M[3] = X[k] * (Y[l] * Z[m + 1]);
-    M[4] = T(0.5) * (X[k + 2] * yz + X[k] * (Y[l + 2] * Z[m] + Y[l] * Z[m + 2] + e2 * yz));
+    M[4] = T(0.5f) * fmaT(X[k + 2], yz, X[k] * fmaT(e2, yz, Y[l + 2] * Z[m] + Y[l] * Z[m + 2]));
 }
 
 template <int k, int l, int m, typename T>
 __device__ __forceinline__ void mcal_a(T M[5], const T *X, const T *Y, const T *Z, T e2, T e4, const T a[5])
 {
 #define YZ(b, c) (Y[l + (b)] * Z[m + (c)])
-    const T h4 = T(0.5) * a[4];
-#define G0(b, c) (a[0] * YZ(b, c) + a[2] * YZ((b) + 1, c) + a[3] * YZ(b, (c) + 1) + \
-                  h4 * (YZ((b) + 2, c) + YZ(b, (c) + 2) + e2 * YZ(b, c)))
-#define GG(p, b, c) (X[k + (p)] * G0(b, c) + (X[k + (p) + 1] * a[1] + X[k + (p) + 2] * h4) * YZ(b, c))
+    const T h4 = T(0.5f) * a[4];
+#define G0(b, c) fmaT(a[0], YZ(b, c), fmaT(a[2], YZ((b) + 1, c), fmaT(a[3], YZ(b, (c) + 1), \
+                  h4 * fmaT(e2, YZ(b, c), YZ((b) + 2, c) + YZ(b, (c) + 2)))))
+#define GG(p, b, c) fmaT(X[k + (p)], G0(b, c), fmaT(X[k + (p) + 1], a[1], X[k + (p) + 2] * h4) * YZ(b, c))
     const T m0 = GG(0, 0, 0);
     M[0] = m0;
     M[1] = GG(1, 0, 0);
     M[2] = GG(0, 1, 0);
     M[3] = GG(0, 0, 1);
-    M[4] = T(0.5) * (GG(2, 0, 0) + GG(0, 2, 0) + GG(0, 0, 2) + e2 * m0 + h4 * (e4 - e2 * e2) * (X[k] * YZ(0, 0)));
+    M[4] = T(0.5f) * (GG(2, 0, 0) + GG(0, 2, 0) + GG(0, 0, 2) +
+                      fmaT(e2, m0, (h4 * (e4 - e2 * e2)) * (X[k] * YZ(0, 0))));
 #undef GG
 #undef G0
 #undef YZ
@@ -166,7 +195,7 @@ __device__ __forceinline__ void add5(T acc[5], const T x[5])
 // lambda.  q = |U|^2 + (K+3)/(2 lambda); kA = pr_factor * 4/(K+3).
 // ---------------------------------------------------------------------------
 template <typename T> struct SlopeFrame {
-    T U0, U1, U2, tl, q, kal2; // tl = 2 lambda, kal2 = kA lambda^2
+    T U0, U1, U2, nU0, nU1, nU2, tl, q, nq, kal2; // tl = 2 lambda, kal2 = kA lambda^2, nX = -X
 };
 
 template <typename T>
@@ -176,24 +205,30 @@ __device__ __forceinline__ SlopeFrame<T> slope_frame(T U0, T U1, T U2, T lam, T 
     f.U0 = U0;
     f.U1 = U1;
     f.U2 = U2;
-    f.tl = T(2) * lam;
-    f.q = U0 * U0 + U1 * U1 + U2 * U2 + T(K + 3) * s;
-    f.kal2 = kA * lam * lam;
+    f.nU0 = -U0;
+    f.nU1 = -U1;
+    f.nU2 = -U2;
+    f.tl = T(2.0f) * lam;
+    f.q = fmaT(U0, U0, fmaT(U1, U1, fmaT(U2, U2, T(float(K + 3)) * s)));
+    f.nq = -f.q;
+    f.kal2 = (kA * lam) * lam;
     return f;
 }
 
 template <typename T>
 __device__ __forceinline__ void slope_solve(const T b[5], const SlopeFrame<T> &f, T a[5])
 {
-    const T R2 = b[1] - f.U0 * b[0];
-    const T R3 = b[2] - f.U1 * b[0];
-    const T R4 = b[3] - f.U2 * b[0];
-    const T R5 = T(2) * b[4] - b[0] * f.q;
-    a[4] = f.kal2 * (R5 - T(2) * (f.U0 * R2 + f.U1 * R3 + f.U2 * R4));
-    a[3] = f.tl * R4 - f.U2 * a[4];
-    a[2] = f.tl * R3 - f.U1 * a[4];
-    a[1] = f.tl * R2 - f.U0 * a[4];
-    a[0] = b[0] - (a[1] * f.U0 + a[2] * f.U1 + a[3] * f.U2) - T(0.5) * a[4] * f.q;
+    const T R2 = fmaT(f.nU0, b[0], b[1]);
+    const T R3 = fmaT(f.nU1, b[0], b[2]);
+    const T R4 = fmaT(f.nU2, b[0], b[3]);
+    const T R5 = fmaT(f.nq, b[0], T(2.0f) * b[4]);
+    const T d = fmaT(f.U0, R2, fmaT(f.U1, R3, f.U2 * R4));
+    a[4] = f.kal2 * fmaT(T(-2.0f), d, R5);
+    a[3] = fmaT(f.nU2, a[4], f.tl * R4);
+    a[2] = fmaT(f.nU1, a[4], f.tl * R3);
+    a[1] = fmaT(f.nU0, a[4], f.tl * R2);
+    const T e = fmaT(a[1], f.U0, fmaT(a[2], f.U1, a[3] * f.U2));
+    a[0] = fmaT(T(-0.5f) * f.q, a[4], b[0] - e);
 }
 
 // ---------------------------------------------------------------------------

@@ -10,6 +10,7 @@
 // in `shift`.
 #include "gks_device.cuh"
 #include "gks_kernels.cuh"
+#include "gks_mixed.cuh"
 #include "../../include/gks_b200.h"
 
 #include <cuda_runtime.h>
@@ -63,11 +64,15 @@ __device__ __forceinline__ unsigned shift(const Cell &x, int dj, int di, int dk)
     return ((unsigned)wrap(x.j + dj, x.nc) * n + (unsigned)wrap(x.i + di, x.nc)) * n + (unsigned)wrap(x.k + dk, x.nc);
 }
 
-// Displacement along the sweep axis: DIR 0 = x (i), 1 = y (j), 2 = z (k).
+// Displacement along the sweep axis: DIR 0 = x (i), 1 = y (j), 2 = z (k);
+// only the swept coordinate wraps.
 template <int DIR>
 __device__ __forceinline__ unsigned along(const Cell &x, int d)
 {
-    return DIR == 0 ? shift(x, 0, d, 0) : (DIR == 1 ? shift(x, d, 0, 0) : shift(x, 0, 0, d));
+    const int n = x.nc;
+    if (DIR == 0) return x.c + (unsigned)((wrap(x.i + d, n) - x.i) * n);
+    if (DIR == 1) return x.c + (unsigned)((wrap(x.j + d, n) - x.j) * n * n);
+    return x.c + (unsigned)(wrap(x.k + d, n) - x.k);
 }
 
 __device__ __forceinline__ double viscosity(const FieldDev &f, double T)
@@ -171,18 +176,18 @@ __device__ __forceinline__ void transverse(const Cell &x, int flags, unsigned &n
                                            unsigned &bk)
 {
     if (DIR == 0) {
-        n = shift(x, 1, 0, 0); s = shift(x, -1, 0, 0);
-        fr = shift(x, 0, 0, 1); bk = shift(x, 0, 0, -1);
+        n = along<1>(x, 1); s = along<1>(x, -1);
+        fr = along<2>(x, 1); bk = along<2>(x, -1);
     } else if (DIR == 1) {
-        n = shift(x, 0, -1, 0); s = shift(x, 0, 1, 0);
-        fr = shift(x, 0, 0, 1); bk = shift(x, 0, 0, -1);
+        n = along<0>(x, -1); s = along<0>(x, 1);
+        fr = along<2>(x, 1); bk = along<2>(x, -1);
     } else {
         if (flags & GKS_FIX_ZSWEEP) {
-            n = shift(x, 1, 0, 0); s = shift(x, -1, 0, 0);
-            fr = shift(x, 0, 1, 0); bk = shift(x, 0, -1, 0);
+            n = along<1>(x, 1); s = along<1>(x, -1);
+            fr = along<0>(x, 1); bk = along<0>(x, -1);
         } else {
-            n = shift(x, 0, 1, 0); s = shift(x, 0, -1, 0);
-            fr = shift(x, 1, 0, 0); bk = shift(x, -1, 0, 0);
+            n = along<0>(x, 1); s = along<0>(x, -1);
+            fr = along<1>(x, 1); bk = along<1>(x, -1);
         }
     }
 }
@@ -296,7 +301,8 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
         fc.kA = f.kA;
         fc.K = f.K;
         double F[5];
-        gks_flux<S>(src, tau0, fc, F);
+        if constexpr (PREC == 0) gks_flux<S>(src, tau0, fc, F);
+        else gks_flux_mixed(src, tau0, fc, F);
         constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
         if (ROT) {
             const double t = F[1];
@@ -321,7 +327,7 @@ __global__ void __launch_bounds__(256) k_update(Batch b)
         if (it - f.base >= f.ncell) continue; // alignment padding after the field
         const Cell x = decode(unsigned(it - f.base), f);
         const unsigned c = x.c;
-        const unsigned cx = shift(x, 0, -1, 0), cy = shift(x, -1, 0, 0), cz = shift(x, 0, 0, -1);
+        const unsigned cx = along<0>(x, -1), cy = along<1>(x, -1), cz = along<2>(x, -1);
         double w[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
