@@ -214,6 +214,78 @@ def cpu_baseline(nc: int, steps: int, warmup: int, planes: int = 8, procs: int =
                       f"{planes}x{nc}x{nc} y-slab of the {nc}^3 field per process, {procs} process(es)"}
 
 
+def ensemble_cases(n_each: int = 32):
+    """96 realisations: n_each at 32^3, 48^3 and 64^3, own seeds, k0 in {3,4,5},
+    Mt uniform in [0.2, 0.5], Re_lambda 72."""
+    import gks_ic
+    import numpy as np
+
+    rng = np.random.default_rng(1234)
+    cases = []
+    seed = 0
+    for nc in (32, 48, 64):
+        for _ in range(n_each):
+            k0 = float(rng.choice([3.0, 4.0, 5.0]))
+            mt = float(rng.uniform(0.2, 0.5))
+            cases.append(gks_ic.make_dhit(nc, k0=k0, Mt=mt, Re_lambda=72.0, seed=seed))
+            seed += 1
+    return cases
+
+
+def run_ensemble(gks, gks_ic, torch, steps: int, warmup: int, local: int, tune: bool) -> dict:
+    cases = ensemble_cases()
+    cells = sum(c.nc ** 3 for c in cases)
+    out = {"fields": len(cases), "sizes": "32x32^3 + 32x48^3 + 32x64^3", "cells_per_step": cells}
+    for name, prec in (("fp64", gks.FP64), ("mixed", gks.MIXED)):
+        s = gks.Solver([gks.phys_from_case(c) for c in cases], prec, device=local)
+        for f, c in enumerate(cases):
+            s.upload(gks_ic.to_conservative_padded(c), f)
+            s.timestep(CFL, f)
+        if tune:
+            s.autotune(2)
+        s.step(warmup)
+        s.sync()
+        ms = timed_steps(s, steps, torch)
+        s.close()
+        out[name] = {"value": cells / (ms * 1e-3), "ms_per_step": ms}
+    out["unit"] = UNIT
+    out["launches_per_step"] = 7
+    return out
+
+
+def run_accuracy(args):
+    """Mixed vs FP64 on the same field to t/t0 = 2: relative errors of the statistics."""
+    import numpy as np
+
+    import gks_b200 as gks
+    import gks_ic
+
+    nc = args.nc
+    case = make_case(nc, 0)
+    W = gks_ic.to_conservative_padded(case)
+    hist = {}
+    for name, prec in (("fp64", gks.FP64), ("mixed", gks.MIXED)):
+        with gks.Solver(gks.phys_from_case(case), prec) as s:
+            s.upload(W)
+            dt = s.timestep(CFL)
+            nsteps = int(np.ceil(2.0 * case.t0 / dt))
+            h = []
+            for k in range(nsteps + 1):
+                if k % 10 == 0 or k == nsteps:
+                    h.append(s.stats())
+                if k < nsteps:
+                    s.step(1)
+            s.sync()
+            hist[name] = h
+    keys = ("tke", "diss", "skew_u", "skew_v", "skew_w")
+    final = {k: abs(hist["mixed"][-1][k] - hist["fp64"][-1][k]) / abs(hist["fp64"][-1][k]) for k in keys}
+    worst = {k: max(abs(a[k] - b[k]) / abs(b[k]) for a, b in zip(hist["mixed"], hist["fp64"])) for k in keys}
+    print(json.dumps({"mode": "accuracy", "nc": nc, "t_over_t0": 2.0, "steps": nsteps, "dt": dt,
+                      "rel_err_final": final, "rel_err_max_over_history": worst,
+                      "tke_fp64_final": hist["fp64"][-1]["tke"], "diss_fp64_final": hist["fp64"][-1]["diss"]}))
+    return 0
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -283,6 +355,25 @@ def run_ours(args):
     for name in solvers:
         solvers[name].close()
 
+    # cost of one diagnostics evaluation (PrintStats' quantities) on the FP64 field
+    s = gks.Solver(phys, gks.FP64, device=local)
+    s.upload(W)
+    s.timestep(CFL)
+    s.stats()
+    t0s = time.perf_counter()
+    for _ in range(3):
+        s.stats()
+    stats_ms = (time.perf_counter() - t0s) / 3 * 1e3
+    s.close()
+
+    ens = None
+    if not args.no_ensemble:
+        ens = run_ensemble(gks, gks_ic, torch, args.steps, args.warmup, local, not args.no_tune)
+        ens["fp64"]["ms_per_step"] = dist.max(ens["fp64"]["ms_per_step"])
+        ens["mixed"]["ms_per_step"] = dist.max(ens["mixed"]["ms_per_step"])
+        for k in ("fp64", "mixed"):
+            ens[k]["value"] = ws * ens["cells_per_step"] / (ens[k]["ms_per_step"] * 1e-3)
+
     # e2e through the reference-facing call: upload from pinned host, step, download
     nt = nc + 6
     host = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True).numpy()
@@ -344,7 +435,8 @@ def run_ours(args):
                          "fp32_peak": peak32},
             "hbm": {"achieved_gbs": BYTES_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e9,
                     "peak_gbs": 6538.0, "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
-            "stage_ms": stages["fp64"], "recon_ms": recon_ms,
+            "stage_ms": stages["fp64"], "recon_ms": recon_ms, "stats_ms": stats_ms,
+            "ensemble": ens,
             "launch": {"fp64": results["fp64"]["launch"], "mixed": results["mixed"]["launch"],
                        "tuned": not args.no_tune},
             "e2e": {"value": ws * cells / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
@@ -369,7 +461,11 @@ def main():
     ap.add_argument("--nc", type=int, default=NC)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-tune", action="store_true", help="keep the untuned launch configuration")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 96-field ensemble line")
+    ap.add_argument("--accuracy", action="store_true", help="mixed vs FP64 statistics to t/t0 = 2, then exit")
     args = ap.parse_args()
+    if args.accuracy:
+        return run_accuracy(args)
     if args.warmup < 3 and args.impl == "ours":
         ap.error("at least 3 warm-up steps")
     if args.impl == "reference":

@@ -14,6 +14,7 @@
 #include "../../include/gks_b200.h"
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <type_traits>
 
 namespace gks {
@@ -573,14 +574,16 @@ __global__ void k_sums2(FieldDev f, const double *means, double *partial)
     block_sums<NSUM2>(acc, partial + (long long)blockIdx.x * NSUM2);
 }
 
-// Sum the per-block partials in a fixed order; optionally divide by ncell.
+// Sum the per-block partials, one warp per quantity, in a fixed order (so the
+// result does not depend on timing); optionally scaled by 1/ncell.
 __global__ void k_finalize(const double *partial, int nblocks, int nsum, double scale, double *out)
 {
-    const int i = threadIdx.x;
+    const int i = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (i >= nsum) return;
     double t = 0.0;
-    for (int bidx = 0; bidx < nblocks; ++bidx) t += partial[(long long)bidx * nsum + i];
-    out[i] = t * scale;
+    for (int bidx = lane; bidx < nblocks; bidx += 32) t += partial[(long long)bidx * nsum + i];
+    t = warp_sum(t);
+    if (lane == 0) out[i] = t * scale;
 }
 
 __global__ void k_check(FieldDev f, int *err)
@@ -702,16 +705,16 @@ cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, cuda
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, cudaStream_t st)
 {
     const int block = 256;
-    const int grid = grid_for(f.ncell, block);
+    const int grid = std::min(grid_for(f.ncell, block), 148 * 8);
     k_velocity<<<grid, block, 0, st>>>(f, scratch);
     const long long lines = (long long)f.nc * f.nc;
     const int lgrid = int((lines + 127) / 128);
     for (int axis = 0; axis < 3; ++axis) k_spline<<<lgrid, 128, 0, st>>>(f, scratch, axis);
     k_sums1<<<grid, block, 0, st>>>(f, scratch, partial);
-    k_finalize<<<1, 32, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
+    k_finalize<<<1, 32 * NSUM1, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
     double *partial2 = partial + (long long)grid * NSUM1;
     k_sums2<<<grid, block, 0, st>>>(f, sums, partial2);
-    k_finalize<<<1, 32, 0, st>>>(partial2, grid, NSUM2, 1.0, sums + NSUM1);
+    k_finalize<<<1, 32 * NSUM2, 0, st>>>(partial2, grid, NSUM2, 1.0, sums + NSUM1);
     return cudaGetLastError();
 }
 
