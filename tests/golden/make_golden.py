@@ -14,6 +14,8 @@ Fixtures
   dhit32.npz     32^3 DHIT of the CPU configuration (k0 4, Mt 0.3, Re 72, seed 0,
                  CFL 0.5): 100-step stats history and printed lines, step-10 field
                  checksums and 4096 sampled cells
+  dhit128.npz    128^3 (same physics, seed 0): 10-step field checksums, 8192 sampled
+                 cells, stats history (python make_golden.py --c1; ~3 min of CPU)
 """
 
 import hashlib
@@ -114,9 +116,25 @@ def interior(W):
     return np.ascontiguousarray(W[:, 3:-3, 3:-3, 3:-3])
 
 
+def c1():
+    """The 128^3 configuration, 10 steps through the reference."""
+    case, r, sha = dhit_run(128, 0, 10, [10])
+    w10 = interior(r["dumps"][10])
+    srng = np.random.default_rng(11)
+    sample = srng.integers(0, 128**3, 8192)
+    flat = w10.reshape(5, -1)
+    np.savez_compressed(
+        os.path.join(HERE, "dhit128.npz"), stats=r["stats"], dt=r["meta"]["dt"], maxval=r["meta"]["maxVAL"],
+        sample_idx=sample, sample_w10=flat[:, sample], sum_w10=flat.sum(1), sumsq_w10=(flat * flat).sum(1),
+        mu0=case.mu0, p0=case.p0, t0=case.t0, Mt=case.Mt, seed=0, nc=128, ic_sha256=sha)
+
+
 def main():
     if not pyoracle.have_ref():
         pyoracle.build()
+    if "--c1" in sys.argv:
+        c1()
+        return
     rng = np.random.default_rng(20240601)
 
     st = weno_stencils(rng)

@@ -99,6 +99,29 @@ def test_fp64_step_matches_reference_32(gks, oracle):
     assert np.all(field_err(W, interior(Wo)) < STEP_RTOL)
 
 
+def test_fp64_step_matches_reference_128(gks):
+    """128^3 (k0 4, Mt 0.3, Re 72, seed 0): 10 steps against the reference's
+    own output (sampled cells, per-component sums and sums of squares)."""
+    g = load("dhit128.npz")
+    case = gks_ic.make_dhit(128, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=0)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(gks_ic.to_conservative_padded(case))
+        dt = s.timestep(0.5)
+        assert dt == float(g["dt"])
+        stats = [s.stats_array()]
+        for _ in range(10):
+            s.step(1)
+            stats.append(s.stats_array())
+        s.sync()
+        W = interior(s.download()).reshape(5, -1)
+    ref = g["sample_w10"]
+    e = np.abs(W[:, g["sample_idx"]] - ref).max(1) / np.abs(ref).max(1)
+    assert np.all(e < STEP_RTOL), e
+    np.testing.assert_allclose(W.sum(1), g["sum_w10"], rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose((W * W).sum(1), g["sumsq_w10"], rtol=1e-12)
+    np.testing.assert_allclose(np.array(stats)[:, :8], g["stats"][:11, 1:9], rtol=STATS_RTOL, atol=1e-13)
+
+
 def test_stats_history_matches_reference_16(gks):
     g = load("dhit16.npz")
     with gks.Solver(gks.phys_from_case(case16(g))) as s:
@@ -278,3 +301,24 @@ def test_call_order_is_enforced(gks):
             s.set_dt(-1.0)
         with pytest.raises(ValueError):
             s.upload(np.zeros((5, 10, 10, 10)))
+
+
+def test_mixed_accuracy_to_two_eddy_times(gks):
+    """Mixed vs FP64 at t/t0 = 2 (64^3, Mt 0.5, Re_lambda 100): KE and dissipation
+    within 1e-5 relative, the precision target of the mixed path."""
+    case = gks_ic.make_dhit(64, k0=4.0, Mt=0.5, Re_lambda=100.0, seed=0)
+    W = gks_ic.to_conservative_padded(case)
+    out, tke0 = {}, None
+    for prec in (gks.FP64, gks.MIXED):
+        with gks.Solver(gks.phys_from_case(case), prec) as s:
+            s.upload(W)
+            tke0 = s.stats()["tke"]
+            dt = s.timestep(0.5)
+            n = int(np.ceil(2.0 * case.t0 / dt))
+            s.step(n)
+            s.sync()
+            out[prec] = s.stats()
+    for key in ("tke", "diss"):
+        a, b = out[gks.MIXED][key], out[gks.FP64][key]
+        assert abs(a - b) < 1e-5 * abs(b), (key, a, b)
+    assert out[gks.FP64]["tke"] < 0.9 * tke0  # the turbulence decayed

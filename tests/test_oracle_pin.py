@@ -74,12 +74,14 @@ def test_printed_rms_columns_16(oracle):
     np.testing.assert_allclose(st[8:11], cols[9:12], rtol=5e-8, atol=1e-20)
 
 
-def test_dhit32_ic_is_the_reference_input():
-    g = load("dhit32.npz")
+@pytest.mark.parametrize("nc", [32, 128])
+def test_dhit_ic_is_the_reference_input(nc):
+    """The committed reference outputs at 32^3 and 128^3 were made from these exact input bytes."""
+    g = load(f"dhit{nc}.npz")
     import hashlib
     import tempfile
 
-    case = gks_ic.make_dhit(32, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=0)
+    case = gks_ic.make_dhit(nc, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=0)
     d = tempfile.mkdtemp()
     gks_ic.write_case(d, case)
     with open(os.path.join(d, "InitialConditions", "params"), "rb") as f:
