@@ -421,7 +421,9 @@ def run_ours(args):
             "data": "synthetic: seeded solenoidal DHIT field (k0 4, Mt 0.5, Re_lambda 100), one replica per GPU",
             "config": {"workload": f"DHIT {nc}^3 WENO-GKS step, FP64 parity path", "nc": nc, "k0": K0,
                        "mach_t": MACH, "re_lambda": RE, "cfl": CFL, "precision": "fp64",
-                       "parallelism": f"replicas x{ws}", "l2": "state 671 MB per field > 126 MB L2, no flush"},
+                       "parallelism": f"replicas x{ws}",
+                       "l2": f"working set {30 * 8 * nc ** 3 / 1e6:.0f} MB per field (state {40 * nc ** 3 / 1e6:.0f} MB)"
+                             " vs 126 MB L2, no flush"},
             "mixed": {"value": mixed_value, "ms_per_step": results["mixed"]["ms"],
                       "speedup_vs_fp64": mixed_value / value,
                       "rel_err_vs_fp64_after_steps": rel, "steps_compared": args.warmup + args.steps,
