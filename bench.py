@@ -167,10 +167,10 @@ def read_traffic(nc: int):
     return None
 
 
-def make_case(nc: int, seed: int):
+def make_case(nc: int, seed: int, mach: float = MACH, re: float = RE):
     import gks_ic
 
-    return gks_ic.make_dhit(nc, k0=K0, Mt=MACH, Re_lambda=RE, seed=seed)
+    return gks_ic.make_dhit(nc, k0=K0, Mt=mach, Re_lambda=re, seed=seed)
 
 
 def timed_steps(solver, steps: int, torch) -> float:
@@ -214,6 +214,30 @@ def cpu_baseline(nc: int, steps: int, warmup: int, planes: int = 8, procs: int =
                       f"{planes}x{nc}x{nc} y-slab of the {nc}^3 field per process, {procs} process(es)"}
 
 
+def reference_gpu(nc: int, steps: int, warmup: int) -> dict | None:
+    """The reference's own GPU path on the same field: GPUupdate.cu and GPUAlloc.cu
+    built for sm_100a (oracle/_ref/ref_gpu_harness).  Each of its steps is evolve()
+    -- host-to-device copy of the padded field, its derivs/flip/flux/update
+    kernels, device-to-host copy -- followed by HaloTransfer on the host; a
+    separate process with its own CUDA context."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gks_ic
+    import pyoracle
+
+    if not pyoracle.have_ref_gpu():
+        return None
+    d = tempfile.mkdtemp(prefix="gks_refgpu_")
+    gks_ic.write_case(d, make_case(nc, 0))
+    try:
+        r = pyoracle.ref_time(d, steps, 1, CFL, warmup, gpu=True, timeout=600)
+    except (subprocess.SubprocessError, OSError, ValueError):
+        return None
+    return {"value": r["cells"] * steps / r["seconds"], "unit": UNIT, "ms_per_step": 1e3 * r["seconds"] / steps,
+            "evolve_ms_per_step": 1e3 * r["step_seconds"] / steps, "steps": steps, "warmup": warmup,
+            "what": "reference GPU path (GPUupdate.cu, nvcc -O3 for sm_100a): evolve() with its per-step "
+                    "host<->device copies of the padded field + host HaloTransfer, wall clock"}
+
+
 def ensemble_cases(n_each: int = 32):
     """96 realisations: n_each at 32^3, 48^3 and 64^3, own seeds, k0 in {3,4,5},
     Mt uniform in [0.2, 0.5], Re_lambda 72."""
@@ -254,21 +278,24 @@ def run_ensemble(gks, gks_ic, torch, steps: int, warmup: int, local: int, tune: 
 
 
 def run_accuracy(args):
-    """Mixed vs FP64 on the same field to t/t0 = 2: relative errors of the statistics."""
+    """Mixed vs FP64 on the same field to t/t0 = args.t_end (statistics every 10
+    steps): relative errors of the statistics, and each precision's step time
+    (CUDA events over 10 further steps)."""
     import numpy as np
+    import torch
 
     import gks_b200 as gks
     import gks_ic
 
     nc = args.nc
-    case = make_case(nc, 0)
+    case = make_case(nc, 0, args.mach, args.re)
     W = gks_ic.to_conservative_padded(case)
-    hist = {}
+    hist, ms = {}, {}
     for name, prec in (("fp64", gks.FP64), ("mixed", gks.MIXED)):
         with gks.Solver(gks.phys_from_case(case), prec) as s:
             s.upload(W)
             dt = s.timestep(CFL)
-            nsteps = int(np.ceil(2.0 * case.t0 / dt))
+            nsteps = int(np.ceil(args.t_end * case.t0 / dt))
             h = []
             for k in range(nsteps + 1):
                 if k % 10 == 0 or k == nsteps:
@@ -277,12 +304,17 @@ def run_accuracy(args):
                     s.step(1)
             s.sync()
             hist[name] = h
+            ms[name] = timed_steps(s, 10, torch)
     keys = ("tke", "diss", "skew_u", "skew_v", "skew_w")
     final = {k: abs(hist["mixed"][-1][k] - hist["fp64"][-1][k]) / abs(hist["fp64"][-1][k]) for k in keys}
     worst = {k: max(abs(a[k] - b[k]) / abs(b[k]) for a, b in zip(hist["mixed"], hist["fp64"])) for k in keys}
-    print(json.dumps({"mode": "accuracy", "nc": nc, "t_over_t0": 2.0, "steps": nsteps, "dt": dt,
+    print(json.dumps({"mode": "accuracy", "nc": nc, "mach_t": args.mach, "re_lambda": args.re,
+                      "t_over_t0": args.t_end, "steps": nsteps, "dt": dt,
                       "rel_err_final": final, "rel_err_max_over_history": worst,
-                      "tke_fp64_final": hist["fp64"][-1]["tke"], "diss_fp64_final": hist["fp64"][-1]["diss"]}))
+                      "tke_fp64_initial": hist["fp64"][0]["tke"], "tke_fp64_final": hist["fp64"][-1]["tke"],
+                      "diss_fp64_final": hist["fp64"][-1]["diss"],
+                      "ms_per_step": ms, "cell_updates_per_s": {k: nc ** 3 / (v * 1e-3) for k, v in ms.items()},
+                      "mixed_speedup": ms["fp64"] / ms["mixed"]}))
     return 0
 
 
@@ -409,9 +441,11 @@ def run_ours(args):
     st64, st32 = results["fp64"]["stats"], results["mixed"]["stats"]
     rel = {k: abs(st32[k] - st64[k]) / abs(st64[k]) for k in ("tke", "diss", "skew_u", "skew_v", "skew_w")}
 
-    cb = None
+    cb = rg = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_baseline(nc, 1, 1, planes=8, procs=1)
+    if rank == 0 and ws == 1 and not args.no_refgpu:
+        rg = reference_gpu(nc, 3, 1)
 
     if rank == 0:
         line = {
@@ -449,6 +483,8 @@ def run_ours(args):
         }
         if cb:
             line["cpu_baseline"] = cb
+        if rg:
+            line["reference_gpu"] = rg
         print(json.dumps(line))
     dist.close()
     return 0
@@ -464,7 +500,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-tune", action="store_true", help="keep the untuned launch configuration")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 96-field ensemble line")
-    ap.add_argument("--accuracy", action="store_true", help="mixed vs FP64 statistics to t/t0 = 2, then exit")
+    ap.add_argument("--no-refgpu", action="store_true", help="skip timing the reference's own GPU path")
+    ap.add_argument("--accuracy", action="store_true", help="mixed vs FP64 statistics to t/t0 = --t-end, then exit")
+    ap.add_argument("--t-end", type=float, default=2.0, help="accuracy run length in eddy turnover times")
+    ap.add_argument("--mach", type=float, default=MACH, help="turbulent Mach number of the accuracy field")
+    ap.add_argument("--re", type=float, default=RE, help="Re_lambda of the accuracy field")
     args = ap.parse_args()
     if args.accuracy:
         return run_accuracy(args)

@@ -432,55 +432,132 @@ __global__ void k_velocity(FieldDev f, double *scr)
     }
 }
 
-// One thread per grid line along `axis`, solving the three velocity
-// components' slope systems with the Thomas algorithm (pivots precomputed):
+// Slopes of the natural cubic spline through the nt = nc + 6 nodes of every
+// padded periodic grid line along `axis` (the reference's einspline over its
+// padded block), for the three velocity components in turn:
 //   2 m0 + m1 = s (f1 - f0);  m_{p-1} + 4 m_p + m_{p+1} = s (f_{p+1} - f_{p-1});
-//   m_{n-2} + 2 m_{n-1} = s (f_{n-1} - f_{n-2}),  s = 3/h.
-// Forward values of interior nodes are parked in the output array and turned
-// into slopes by the backward pass.
-__global__ void k_spline(FieldDev f, double *scr, int axis)
+//   m_{n-2} + 2 m_{n-1} = s (f_{n-1} - f_{n-2}),  s = 3/h,
+// solved per line by the Thomas algorithm with precomputed pivots.  One warp
+// owns 32 lines, one lane per line.  Values move through a per-warp shared
+// tile 32 nodes at a time, so that every global access is a coalesced row
+// (along the line for axis 2, across lines otherwise) and a chunk's loads are
+// all in flight together instead of one dependent load per node.  Forward
+// values of interior nodes are parked in the output array and turned into
+// slopes by the backward pass.
+constexpr int kSplLines = 32, kSplChunk = 32, kSplPitch = kSplChunk + 3, kSplWarps = 4;
+
+__global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *scr, int axis)
 {
+    __shared__ double tiles[kSplWarps][kSplLines][kSplPitch];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double (*tile)[kSplPitch] = tiles[wid];
     const int nc = f.nc, nt = nc + 6;
     const long long n = f.ncell;
     const long long lines = (long long)nc * nc;
-    const long long line = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (line >= lines) return;
-    const int a = int(line / nc), bb = int(line % nc);
-    long long base, st;
-    if (axis == 0) { base = (long long)a * nc + bb; st = (long long)nc * nc; }        // along j, (i,k) = (a,b)
-    else if (axis == 1) { base = (long long)a * nc * nc + bb; st = nc; }              // along i, (j,k)
-    else { base = ((long long)a * nc + bb) * nc; st = 1; }                           // along k, (j,i)
+    const long long line0 = ((long long)blockIdx.x * kSplWarps + wid) * kSplLines;
+    if (line0 >= lines) return; // uniform per warp
+    const int nl = int(min((long long)kSplLines, lines - line0));
+    const long long st = axis == 0 ? (long long)nc * nc : (axis == 1 ? (long long)nc : 1LL);
+    auto base_of = [&](int l) -> long long {
+        const long long L = line0 + l;
+        const long long a = L / nc, b = L % nc;
+        return axis == 0 ? a * nc + b : (axis == 1 ? a * nc * nc + b : (a * nc + b) * nc); // (i,k), (j,k), (j,i)
+    };
+    const bool mine = lane < nl;
+    const long long mybase = base_of(mine ? lane : 0);
     const double s = f.spl_s;
     const double *cp = f.spl_cp, *inv = f.spl_inv;
+    // node p of a line sits at cell wrap(p - 3) along the axis
+    auto node_off = [&](int p) -> long long { return (long long)wrap(p - 3, nc) * st; };
+
 #pragma unroll 1
     for (int comp = 0; comp < 3; ++comp) {
         const double *u = scr + comp * n;
         double *g = scr + (3 + 3 * comp + axis) * n;
-        auto val = [&](int p) { return u[base + (long long)wrap(p - 3, nc) * st]; };
-        double fm = val(0), f0 = fm, fp = val(1);
-        double dp = (s * (fp - f0)) * inv[0];
-        double dlast[3];
-        for (int p = 1; p < nt; ++p) {
-            fm = f0;
-            f0 = fp;
-            double r;
-            if (p < nt - 1) {
-                fp = val(p + 1);
-                r = s * (fp - fm);
-            } else {
-                r = s * (f0 - fm);
+        double dp = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0; // d0..d2: forward values of the last three nodes
+        // forward pass: tile column jj holds node p0 - 1 + jj, jj = 0 .. 33
+#pragma unroll 1
+        for (int p0 = 0; p0 < nt; p0 += kSplChunk) {
+            if (axis == 2) {
+                for (int l = 0; l < nl; ++l) {
+                    const long long b = base_of(l);
+                    for (int jj = lane; jj < kSplChunk + 2; jj += 32) {
+                        const int p = p0 - 1 + jj;
+                        if (p >= 0 && p < nt) tile[l][jj] = u[b + node_off(p)];
+                    }
+                }
+            } else if (mine) {
+#pragma unroll 4
+                for (int jj = 0; jj < kSplChunk + 2; ++jj) {
+                    const int p = p0 - 1 + jj;
+                    if (p >= 0 && p < nt) tile[lane][jj] = u[mybase + node_off(p)];
+                }
             }
-            dp = (r - dp) * inv[p];
-            if (p >= 3 && p <= nt - 4) g[base + (long long)(p - 3) * st] = dp;
-            else if (p >= nt - 3) dlast[p - (nt - 3)] = dp;
+            __syncwarp();
+            if (mine) {
+                const int cend = min(kSplChunk, nt - p0);
+                for (int c = 0; c < cend; ++c) {
+                    const int p = p0 + c, jj = c + 1;
+                    if (p == 0) {
+                        dp = (s * (tile[lane][jj + 1] - tile[lane][jj])) * inv[0];
+                    } else {
+                        const double r = p < nt - 1 ? s * (tile[lane][jj + 1] - tile[lane][jj - 1])
+                                                    : s * (tile[lane][jj] - tile[lane][jj - 1]);
+                        dp = (r - dp) * inv[p];
+                    }
+                    if (p == nt - 3) d0 = dp;
+                    else if (p == nt - 2) d1 = dp;
+                    else if (p == nt - 1) d2 = dp;
+                    tile[lane][c] = dp; // column c (node p - 1) is no longer read
+                }
+            }
+            __syncwarp();
+            // park forward values of nodes 3 .. nt-4 at cell p - 3
+            if (axis == 2) {
+                for (int l = 0; l < nl; ++l) {
+                    const long long b = base_of(l);
+                    const int p = p0 + lane;
+                    if (p >= 3 && p <= nt - 4) g[b + (long long)(p - 3)] = tile[l][lane];
+                }
+            } else if (mine) {
+#pragma unroll 4
+                for (int c = 0; c < kSplChunk; ++c) {
+                    const int p = p0 + c;
+                    if (p >= 3 && p <= nt - 4) g[mybase + (long long)(p - 3) * st] = tile[lane][c];
+                }
+            }
+            __syncwarp();
         }
-        double m = dlast[2];
-        m = dlast[1] - cp[nt - 2] * m;
-        m = dlast[0] - cp[nt - 3] * m;
-        for (int p = nt - 4; p >= 3; --p) {
-            const long long o = base + (long long)(p - 3) * st;
-            m = g[o] - cp[p] * m;
-            g[o] = m;
+        // backward pass over cells q = p - 3 = nc-1 .. 0, in chunks from the top
+        double m = d2;
+        m = d1 - cp[nt - 2] * m;
+        m = d0 - cp[nt - 3] * m;
+#pragma unroll 1
+        for (int q0 = ((nc - 1) / kSplChunk) * kSplChunk; q0 >= 0; q0 -= kSplChunk) {
+            const int cnt = min(kSplChunk, nc - q0);
+            if (axis == 2) {
+                for (int l = 0; l < nl; ++l)
+                    if (lane < cnt) tile[l][lane] = g[base_of(l) + (long long)(q0 + lane)];
+            } else if (mine) {
+#pragma unroll 4
+                for (int c = 0; c < cnt; ++c) tile[lane][c] = g[mybase + (long long)(q0 + c) * st];
+            }
+            __syncwarp();
+            if (mine) {
+                for (int c = cnt - 1; c >= 0; --c) {
+                    m = tile[lane][c] - cp[q0 + c + 3] * m;
+                    tile[lane][c] = m;
+                }
+            }
+            __syncwarp();
+            if (axis == 2) {
+                for (int l = 0; l < nl; ++l)
+                    if (lane < cnt) g[base_of(l) + (long long)(q0 + lane)] = tile[l][lane];
+            } else if (mine) {
+#pragma unroll 4
+                for (int c = 0; c < cnt; ++c) g[mybase + (long long)(q0 + c) * st] = tile[lane][c];
+            }
+            __syncwarp();
         }
     }
 }
@@ -708,8 +785,9 @@ cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, do
     const int grid = std::min(grid_for(f.ncell, block), 148 * 8);
     k_velocity<<<grid, block, 0, st>>>(f, scratch);
     const long long lines = (long long)f.nc * f.nc;
-    const int lgrid = int((lines + 127) / 128);
-    for (int axis = 0; axis < 3; ++axis) k_spline<<<lgrid, 128, 0, st>>>(f, scratch, axis);
+    const int lper = kSplLines * kSplWarps;
+    const int lgrid = int((lines + lper - 1) / lper);
+    for (int axis = 0; axis < 3; ++axis) k_spline<<<lgrid, 32 * kSplWarps, 0, st>>>(f, scratch, axis);
     k_sums1<<<grid, block, 0, st>>>(f, scratch, partial);
     k_finalize<<<1, 32 * NSUM1, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
     double *partial2 = partial + (long long)grid * NSUM1;

@@ -5,7 +5,9 @@ Two checkers live under oracle/:
 * ``build/liboracle.so``: the plain-C restatement of the reference hot path
   (gks_oracle.c), loaded through ctypes;
 * ``_ref/ref_harness``: the reference's own CPU path compiled from its sources
-  (see the Makefile), driven as a subprocess.
+  (see the Makefile), driven as a subprocess;
+* ``_ref/ref_gpu_harness``: the same driver around the reference's own GPU
+  path (GPUupdate.cu, GPUAlloc.cu) built for sm_100a; it needs a GPU.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this
 module, and only to check or time against; the product never imports it.
@@ -25,6 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
 REF_HARNESS_FAST = os.path.join(HERE, "_ref", "ref_harness_fast")
+REF_GPU_HARNESS = os.path.join(HERE, "_ref", "ref_gpu_harness")
 
 VISC_SUTHERLAND = 0
 VISC_POWER = 1
@@ -135,12 +138,17 @@ def have_ref() -> bool:
     return os.path.exists(REF_HARNESS)
 
 
-def ref_run(casedir: str, nsteps: int, cfl: float, dumps, stats_on=True, outdir=None):
-    """Run the reference binary; returns dict(meta, stats, dumps, stdout)."""
+def have_ref_gpu() -> bool:
+    return os.path.exists(REF_GPU_HARNESS)
+
+
+def ref_run(casedir: str, nsteps: int, cfl: float, dumps, stats_on=True, outdir=None, gpu=False):
+    """Run the reference binary (its CPU path, or with gpu=True its GPU path);
+    returns dict(meta, stats, dumps, stdout)."""
     outdir = outdir or tempfile.mkdtemp(prefix="gksref_")
     os.makedirs(outdir, exist_ok=True)
     dl = ",".join(str(d) for d in dumps) if dumps else ","
-    cp = subprocess.run([REF_HARNESS, "run", os.path.abspath(casedir), os.path.abspath(outdir), str(nsteps),
+    cp = subprocess.run([REF_GPU_HARNESS if gpu else REF_HARNESS, "run", os.path.abspath(casedir), os.path.abspath(outdir), str(nsteps),
                          repr(cfl), "1" if stats_on else "0", dl],
                         check=True, capture_output=True, text=True)
     meta = {}
@@ -182,13 +190,14 @@ def ref_flux(inputs: np.ndarray, gam=1.4, K=2):
     return np.fromfile(os.path.join(d, "out"), dtype=np.float64).reshape(n, 5)
 
 
-def ref_time_cmd(casedir: str, nsteps: int, slabs: int, cfl: float, warmup: int = 0, fast=True) -> list:
-    exe = REF_HARNESS_FAST if fast else REF_HARNESS
+def ref_time_cmd(casedir: str, nsteps: int, slabs: int, cfl: float, warmup: int = 0, fast=True, gpu=False) -> list:
+    exe = REF_GPU_HARNESS if gpu else (REF_HARNESS_FAST if fast else REF_HARNESS)
     return [exe, "time", os.path.abspath(casedir), str(nsteps), str(slabs), repr(cfl), str(warmup)]
 
 
-def ref_time(casedir: str, nsteps: int, slabs: int, cfl: float, warmup: int = 0, fast=True) -> dict:
+def ref_time(casedir: str, nsteps: int, slabs: int, cfl: float, warmup: int = 0, fast=True, gpu=False,
+             timeout=None) -> dict:
     import json
-    cp = subprocess.run(ref_time_cmd(casedir, nsteps, slabs, cfl, warmup, fast), check=True, capture_output=True,
-                        text=True)
+    cp = subprocess.run(ref_time_cmd(casedir, nsteps, slabs, cfl, warmup, fast, gpu), check=True,
+                        capture_output=True, text=True, timeout=timeout)
     return json.loads(cp.stdout.strip().splitlines()[-1])

@@ -25,6 +25,14 @@
  *        process grid after [warmup] untimed steps; prints one JSON line.
  *   weno <in> <out>   ApplyWENO (update.cpp:502-625) on packed stencils.
  *   flux <in> <out>   flux (GKMflux.cpp:11-215) on packed interface states.
+ *
+ * Built with -DUseGPU (oracle/_ref/ref_gpu_harness) the same driver runs the
+ * reference's own GPU path instead: update.cpp with -DUseGPU, GPUupdate.cu and
+ * GPUAlloc.cu compiled for sm_100a with the reference makefile's nvcc flags
+ * (weno/makefileGPU:27-31, arch changed).  evolveEulerian(W, dev) (update.cpp:
+ * 179-183) then calls evolve (GPUupdate.cu:65-196), which copies the padded
+ * field to the device, runs derivs/flip/flux/update kernels and copies it back.
+ * Modes run and time only.
  */
 #include <mpi.h>
 
@@ -40,6 +48,9 @@
 #include "GKMflux.h"
 #include "param.h"
 #include "update.h"
+#ifdef UseGPU
+#include <cuda_runtime.h>
+#endif
 
 /* File-scope globals of weno/src/update.cpp:7-33 read and written here. */
 extern ptype dt, t, maxVAL;
@@ -66,6 +77,52 @@ struct Halo {
         HaloTransfer(W, sW.data(), rW.data(), sE.data(), rE.data(), sS.data(), rS.data(), sN.data(),
                      rN.data(), sB.data(), rB.data(), sF.data(), rF.data());
     }
+};
+
+/* One step of the reference's hot path, as Evolve calls it (update.cpp:131-137). */
+struct Stepper {
+#ifdef UseGPU
+    DevAlloc *dev = nullptr;
+    void init()
+    {
+        dev = new DevAlloc(); /* GPUAlloc.cu:3-17: 50 unchecked cudaMallocs */
+        ptype *all[] = {dev->d_W0, dev->d_W1, dev->d_W2, dev->d_W3, dev->d_W4, dev->d_F0x, dev->d_F1x,
+                        dev->d_F2x, dev->d_F3x, dev->d_F4x, dev->d_F0y, dev->d_F1y, dev->d_F2y, dev->d_F3y,
+                        dev->d_F4y, dev->d_F0z, dev->d_F1z, dev->d_F2z, dev->d_F3z, dev->d_F4z, dev->d_DW0xl,
+                        dev->d_DW1xl, dev->d_DW2xl, dev->d_DW3xl, dev->d_DW4xl, dev->d_DW0yl, dev->d_DW1yl,
+                        dev->d_DW2yl, dev->d_DW3yl, dev->d_DW4yl, dev->d_DW0zl, dev->d_DW1zl, dev->d_DW2zl,
+                        dev->d_DW3zl, dev->d_DW4zl, dev->d_DW0xr, dev->d_DW1xr, dev->d_DW2xr, dev->d_DW3xr,
+                        dev->d_DW4xr, dev->d_DW0yr, dev->d_DW1yr, dev->d_DW2yr, dev->d_DW3yr, dev->d_DW4yr,
+                        dev->d_DW0zr, dev->d_DW1zr, dev->d_DW2zr, dev->d_DW3zr, dev->d_DW4zr};
+        /* refuse to launch anything on a failed allocation */
+        const cudaError_t e = cudaGetLastError();
+        for (ptype *a : all)
+            if (a == nullptr || e != cudaSuccess) {
+                fprintf(stderr, "DevAlloc failed: %s\n", cudaGetErrorString(e));
+                exit(3);
+            }
+    }
+    void step(ptype *W[5])
+    {
+        evolveEulerian(W, dev);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            fprintf(stderr, "reference GPU step failed: %s\n", cudaGetErrorString(e));
+            exit(3);
+        }
+    }
+#else
+    ptype *Fx[5], *Fy[5], *Fz[5];
+    void init()
+    {
+        for (int q = 0; q < 5; ++q) {
+            Fx[q] = new ptype[Nt_seg]();
+            Fy[q] = new ptype[Nt_seg]();
+            Fz[q] = new ptype[Nt_seg]();
+        }
+    }
+    void step(ptype *W[5]) { evolveEulerian(W, Fx, Fy, Fz); }
+#endif
 };
 
 void setup_block(int slabs)
@@ -115,12 +172,8 @@ int mode_run(int argc, char **argv)
     setup_block(1);
     ptype *W[5];
     for (int q = 0; q < 5; ++q) W[q] = new ptype[Nt_seg]();
-    ptype *Fx[5], *Fy[5], *Fz[5];
-    for (int q = 0; q < 5; ++q) {
-        Fx[q] = new ptype[Nt_seg]();
-        Fy[q] = new ptype[Nt_seg]();
-        Fz[q] = new ptype[Nt_seg]();
-    }
+    Stepper stepper;
+    stepper.init();
     ptype *den = new ptype[Nt_seg], *u = new ptype[Nt_seg], *v = new ptype[Nt_seg],
           *w = new ptype[Nt_seg], *p = new ptype[Nt_seg];
     UBspline_3d_d *splinep[5];
@@ -151,7 +204,7 @@ int mode_run(int argc, char **argv)
     for (int s = 0; s < nsteps; ++s) {
         if (do_stats) stats();
         dump(s);
-        evolveEulerian(W, Fx, Fy, Fz);
+        stepper.step(W);
         halo.exchange(W);
         t += dt;
         iter++;
@@ -178,13 +231,10 @@ int mode_time(int argc, char **argv)
     const int warmup = argc > 6 ? atoi(argv[6]) : 0;
     if (chdir(argv[2]) != 0) { perror("chdir"); return 2; }
     setup_block(slabs);
-    ptype *W[5], *Fx[5], *Fy[5], *Fz[5];
-    for (int q = 0; q < 5; ++q) {
-        W[q] = new ptype[Nt_seg]();
-        Fx[q] = new ptype[Nt_seg]();
-        Fy[q] = new ptype[Nt_seg]();
-        Fz[q] = new ptype[Nt_seg]();
-    }
+    ptype *W[5];
+    for (int q = 0; q < 5; ++q) W[q] = new ptype[Nt_seg]();
+    Stepper stepper;
+    stepper.init();
     Halo halo;
     halo.alloc();
     Initialize_DHIT(W);
@@ -192,22 +242,24 @@ int mode_time(int argc, char **argv)
     timestep(W);
     if (cfl_run > 0) dt = cfl_run * dx / maxVAL;
     for (int s = 0; s < warmup; ++s) {
-        evolveEulerian(W, Fx, Fy, Fz);
+        stepper.step(W);
         halo.exchange(W);
     }
-    std::vector<double> secs;
+    double tot = 0, tstep = 0;
     for (int s = 0; s < nsteps; ++s) {
         auto a = std::chrono::steady_clock::now();
-        evolveEulerian(W, Fx, Fy, Fz);
+        stepper.step(W);
+        auto m = std::chrono::steady_clock::now();
         halo.exchange(W);
         auto b = std::chrono::steady_clock::now();
-        secs.push_back(std::chrono::duration<double>(b - a).count());
+        tot += std::chrono::duration<double>(b - a).count();
+        tstep += std::chrono::duration<double>(m - a).count();
     }
-    double tot = 0;
-    for (double x : secs) tot += x;
+    /* seconds: step + halo exchange; step_seconds: evolveEulerian alone (on the GPU
+     * path: evolve, i.e. its host<->device copies and kernels) */
     printf("{\"cells\": %d, \"nc\": %d, \"slab\": [%d, %d, %d], \"steps\": %d, \"seconds\": %.9g, "
-           "\"cell_updates_per_s\": %.9g}\n",
-           Nc_seg, nc, nc_segy, nc_segx, nc_segz, nsteps, tot, (double)Nc_seg * nsteps / tot);
+           "\"step_seconds\": %.9g, \"cell_updates_per_s\": %.9g}\n",
+           Nc_seg, nc, nc_segy, nc_segx, nc_segz, nsteps, tot, tstep, (double)Nc_seg * nsteps / tot);
     return 0;
 }
 
@@ -227,6 +279,7 @@ std::vector<double> read_blob(const char *path, int &n, std::vector<double> &hdr
     return rest;
 }
 
+#ifdef UseCPU
 int mode_weno(int argc, char **argv)
 {
     if (argc < 4) return 2;
@@ -277,6 +330,7 @@ int mode_flux(int argc, char **argv)
     fclose(f);
     return 0;
 }
+#endif
 
 } // namespace
 
@@ -289,8 +343,10 @@ int main(int argc, char **argv)
     const std::string mode = argv[1];
     if (mode == "run") return mode_run(argc, argv);
     if (mode == "time") return mode_time(argc, argv);
+#ifdef UseCPU
     if (mode == "weno") return mode_weno(argc, argv);
     if (mode == "flux") return mode_flux(argc, argv);
+#endif
     fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;
 }

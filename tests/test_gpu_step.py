@@ -122,6 +122,32 @@ def test_fp64_step_matches_reference_128(gks):
     np.testing.assert_allclose(np.array(stats)[:, :8], g["stats"][:11, 1:9], rtol=STATS_RTOL, atol=1e-13)
 
 
+@pytest.mark.parametrize("nc", [16, 32])
+def test_gpu_semantics_match_reference_gpu_path(gks, nc):
+    """GKS_DIRECT_ENERGY with pr_factor 1 against the reference's own GPU path
+    (GPUupdate.cu built for sm_100a and run on a B200, refgpu*.npz): 10 steps."""
+    g = load(f"refgpu{nc}.npz")
+    case = gks_ic.make_dhit(nc, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=int(g["seed"]))
+    phys = gks.phys_from_case(case, pr_factor=gks.PR_FACTOR_GPU)
+    with gks.Solver(phys, gks.FP64, gks.DIRECT_ENERGY) as s:
+        s.upload(gks_ic.to_conservative_padded(case))
+        dt = s.timestep(0.5)
+        assert dt == float(g["dt"])
+        stats = [s.stats_array()]
+        for _ in range(10):
+            s.step(1)
+            stats.append(s.stats_array())
+        s.sync()
+        W = interior(s.download()).reshape(5, -1)
+    if nc == 16:
+        assert np.all(field_err(W, g["w10"]) < STEP_RTOL)
+    else:
+        ref = g["sample_w10"]
+        assert np.all(np.abs(W[:, g["sample_idx"]] - ref).max(1) / np.abs(ref).max(1) < STEP_RTOL)
+        np.testing.assert_allclose(W.sum(1), g["sum_w10"], rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(np.array(stats)[:, :8], g["stats"][:11, 1:9], rtol=STATS_RTOL, atol=1e-13)
+
+
 def test_stats_history_matches_reference_16(gks):
     g = load("dhit16.npz")
     with gks.Solver(gks.phys_from_case(case16(g))) as s:

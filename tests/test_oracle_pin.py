@@ -104,6 +104,57 @@ def test_dhit32_ten_steps_match_reference(oracle):
     assert np.array_equal(flat.sum(1), g["sum_w10"])
 
 
+def _err(a, b):
+    a = a.reshape(5, -1)
+    b = b.reshape(5, -1)
+    return np.abs(a - b).max(1) / np.abs(b).max(1)
+
+
+def test_gpu_semantics_match_reference_gpu_path(oracle):
+    """The oracle's reference-GPU mode (direct-energy WENO, no 1/Pr) against the
+    reference's own GPU path run on a B200 (refgpu*.npz, make_golden_refgpu.py):
+    CUDA's FMA contraction and math library against the C restatement, so the
+    bar is the 1e-12 relative parity tolerance, not bit equality."""
+    g = load("refgpu16.npz")
+    case = gks_ic.make_dhit(16, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=1)
+    prm = oracle.params(16, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0, pr_factor=oracle.PR_FACTOR_GPU,
+                        flags=oracle.DIRECT_ENERGY)
+    W = gks_ic.to_conservative_padded(case)
+    dt = 0.5 * prm.dx / oracle.maxval(W, prm)
+    assert dt == float(g["dt"])
+    stats = [oracle.stats(W, prm)]
+    oracle.step(W, prm, dt, 1)
+    assert np.all(_err(W[:, 3:-3, 3:-3, 3:-3], g["w1"]) < 1e-12)
+    for _ in range(9):
+        stats.append(oracle.stats(W, prm))
+        oracle.step(W, prm, dt, 1)
+    stats.append(oracle.stats(W, prm))
+    assert np.all(_err(W[:, 3:-3, 3:-3, 3:-3], g["w10"]) < 1e-12)
+    np.testing.assert_allclose(np.array(stats)[:, :8], g["stats"][:, 1:9], rtol=1e-10, atol=1e-13)
+
+    g = load("refgpu32.npz")
+    case = gks_ic.make_dhit(32, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=0)
+    prm = oracle.params(32, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0, pr_factor=oracle.PR_FACTOR_GPU,
+                        flags=oracle.DIRECT_ENERGY)
+    W = gks_ic.to_conservative_padded(case)
+    oracle.step(W, prm, float(g["dt"]), 10)
+    flat = W[:, 3:-3, 3:-3, 3:-3].reshape(5, -1)
+    ref = g["sample_w10"]
+    assert np.all(np.abs(flat[:, g["sample_idx"]] - ref).max(1) / np.abs(ref).max(1) < 1e-12)
+    np.testing.assert_allclose(flat.sum(1), g["sum_w10"], rtol=1e-12, atol=1e-9)
+
+
+def test_gpu_and_cpu_semantics_differ(oracle):
+    """The two reference paths are different schemes: the CPU-mode oracle is far
+    from the reference GPU output (so the test above is not vacuous)."""
+    g = load("refgpu16.npz")
+    case = gks_ic.make_dhit(16, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=1)
+    prm = oracle.params(16, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    W = gks_ic.to_conservative_padded(case)
+    oracle.step(W, prm, float(g["dt"]), 1)
+    assert np.all(_err(W[:, 3:-3, 3:-3, 3:-3], g["w1"]) > 1e-4)
+
+
 def test_known_answer_weno_exact_on_constant_and_linear(oracle):
     g = load("weno_ref.npz")
     st = g["stencils"]
