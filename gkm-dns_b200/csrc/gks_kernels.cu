@@ -9,8 +9,8 @@
 // reference (HaloTransfer on one rank, update.cpp:894-1054) is the index wrap
 // in `shift`.
 #include "gks_device.cuh"
+#include "gks_flux.cuh"
 #include "gks_kernels.cuh"
-#include "gks_mixed.cuh"
 #include "../../include/gks_b200.h"
 
 #include <cuda_runtime.h>
@@ -219,7 +219,8 @@ struct SweepSrc {
     __device__ __forceinline__ void load(const FieldDev &f, unsigned c, unsigned c1, unsigned cn, unsigned cs,
                                          unsigned cf, unsigned cb)
     {
-        const double idx = f.inv_dx, ys = DIR == 1 ? -0.5 : 0.5;
+        // differences in double (they cancel), scaled in S
+        const S kn = S(2.0 * f.inv_dx), kt = S(0.5 * f.inv_dx), ky = DIR == 1 ? -kt : kt;
         const int t = threadIdx.x;
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -228,12 +229,12 @@ struct SweepSrc {
             const double wL = __ldg(f.W[o] + c), wR = __ldg(f.W[o] + c1);
             Wl[q] = __ldg(rl + c);
             Wr[q] = __ldg(rr + c);
-            DWl[0][q] = S(2.0 * (Wl[q] - wL) * idx);
-            DWl[1][q] = S(ys * (__ldg(rl + cn) - __ldg(rl + cs)) * idx);
-            DWl[2][q] = S(0.5 * (__ldg(rl + cf) - __ldg(rl + cb)) * idx);
-            park_dw[q][t] = S(2.0 * (wR - Wr[q]) * idx);
-            park_dw[5 + q][t] = S(ys * (__ldg(rr + cn) - __ldg(rr + cs)) * idx);
-            park_dw[10 + q][t] = S(0.5 * (__ldg(rr + cf) - __ldg(rr + cb)) * idx);
+            DWl[0][q] = kn * S(Wl[q] - wL);
+            DWl[1][q] = ky * S(__ldg(rl + cn) - __ldg(rl + cs));
+            DWl[2][q] = kt * S(__ldg(rl + cf) - __ldg(rl + cb));
+            park_dw[q][t] = kn * S(wR - Wr[q]);
+            park_dw[5 + q][t] = ky * S(__ldg(rr + cn) - __ldg(rr + cs));
+            park_dw[10 + q][t] = kt * S(__ldg(rr + cf) - __ldg(rr + cb));
             park_w[q][t] = wL;
             park_w[5 + q][t] = wR;
         }
@@ -302,8 +303,7 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
         fc.kA = f.kA;
         fc.K = f.K;
         double F[5];
-        if constexpr (PREC == 0) gks_flux<S>(src, tau0, fc, F);
-        else gks_flux_mixed(src, tau0, fc, F);
+        gks_flux<S>(src, tau0, fc, F);
         constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
         if (ROT) {
             const double t = F[1];
