@@ -143,7 +143,7 @@ int read_err(gks_ctx *ctx, int *word, bool clear)
 gks::LaunchCfg persistent(gks_ctx *ctx, int kind, int dir, int variant, int mult)
 {
     gks::LaunchCfg c;
-    c.block = kind == gks::K_UPDATE ? 256 : 128;
+    c.block = kind == gks::K_UPDATE ? gks::kUpdateBlock : (kind == gks::K_FLUX ? gks::kFluxBlock : gks::kReconBlock);
     c.variant = variant;
     int per_sm = 1;
     if (gks::max_resident_blocks(kind, dir, ctx->precision, variant, c.block, &per_sm) != cudaSuccess || per_sm < 1)
@@ -630,6 +630,20 @@ int gks_get_launch(gks_ctx *ctx, int kind, int dir, int *block, int *grid, int *
     if (block) *block = c.block;
     if (grid) *grid = c.grid;
     if (variant) *variant = c.variant;
+    return GKS_OK;
+}
+
+int gks_set_launch(gks_ctx *ctx, int kind, int dir, int grid, int variant)
+{
+    if (!ctx || kind < 0 || kind >= gks::K_KINDS || dir < 0 || dir > 2) return GKS_EINVAL;
+    const int nvar = kind == gks::K_RECON ? gks::kReconVariants : (kind == gks::K_FLUX ? gks::kFluxVariants : 1);
+    if (variant < 0 || variant >= nvar) return fail(ctx, GKS_EINVAL, "no such kernel variant");
+    if (grid < 0) return fail(ctx, GKS_EINVAL, "negative grid");
+    CK(cudaSetDevice(ctx->device));
+    gks::LaunchCfg c = persistent(ctx, kind, dir, variant, 1);
+    if (grid > 0) c.grid = grid;
+    ctx->cfg[kind][dir] = c;
+    drop_graph(ctx);
     return GKS_OK;
 }
 

@@ -4,7 +4,10 @@
 // (GKMflux.cpp:301-308) and the arithmetic helpers the flux (gks_flux.cuh)
 // is written with.  The algebra is the reference's; the evaluation order is
 // this file's own (one reciprocal per WENO side instead of eight divisions),
-// so results agree with the reference to rounding, not bit for bit.
+// so results agree with the reference to rounding, not bit for bit.  Every
+// fused multiply-add is written out (the kernels are compiled without
+// implicit contraction), so results do not depend on how the compiler
+// schedules a particular register-cap variant.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,11 +37,22 @@ __device__ __forceinline__ f2 operator*(f2 a, f2 b) { f2 r; r.v = __fmul2_rn(a.v
 __device__ __forceinline__ f2 operator-(f2 a, f2 b) { f2 r; r.v = __ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v); return r; }
 __device__ __forceinline__ f2 operator-(f2 a) { f2 r; r.v = __fmul2_rn(a.v, make_float2(-1.f, -1.f)); return r; }
 __device__ __forceinline__ f2 &operator+=(f2 &a, f2 b) { a = a + b; return a; }
+__device__ __forceinline__ f2 &operator-=(f2 &a, f2 b) { a = a - b; return a; }
+__device__ __forceinline__ f2 &operator*=(f2 &a, f2 b) { a = a * b; return a; }
 
 // a*b + c with one rounding, for every arithmetic type used here.
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ f2 fmaT(f2 a, f2 b, f2 c) { f2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r; }
+
+template <> __device__ __forceinline__ f2 rcp<f2>(f2 x) { return f2(__frcp_rn(x.v.x), __frcp_rn(x.v.y)); }
+__device__ __forceinline__ double fmaxT(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float fmaxT(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ f2 fmaxT(f2 a, f2 b) { return f2(fmaxf(a.v.x, b.v.x), fmaxf(a.v.y, b.v.y)); }
+
+// A constant in type T (rounded once from its double value).
+template <typename T> __device__ __forceinline__ constexpr T cst(double x) { return T(x); }
+template <> __device__ __forceinline__ f2 cst<f2>(double x) { return f2(float(x)); }
 
 // ---------------------------------------------------------------------------
 // WENO-SYMOO on one scalar 6-point stencil (update.cpp:505-557): four cubic
@@ -53,29 +67,31 @@ __device__ __forceinline__ f2 fmaT(f2 a, f2 b, f2 c) { f2 r; r.v = __ffma2_rn(a.
 template <typename T>
 __device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1, T q2, T q3, T eps)
 {
-    const T third = T(1) / T(3), sixth = T(1) / T(6);
-    const T p0 = third * a - (T(7) * sixth) * b + (T(11) * sixth) * c;
-    const T p1 = -sixth * b + (T(5) * sixth) * c + third * d;
-    const T p2 = third * c + (T(5) * sixth) * d - sixth * e;
-    const T p3 = (T(11) * sixth) * d - (T(7) * sixth) * e + third * f;
+    const T third = cst<T>(1.0 / 3.0), msixth = cst<T>(-1.0 / 6.0);
+    const T ms7 = cst<T>(-7.0 / 6.0), s11 = cst<T>(11.0 / 6.0), s5 = cst<T>(5.0 / 6.0);
+    const T p0 = fmaT(third, a, fmaT(ms7, b, s11 * c));
+    const T p1 = fmaT(msixth, b, fmaT(s5, c, third * d));
+    const T p2 = fmaT(third, c, fmaT(s5, d, msixth * e));
+    const T p3 = fmaT(s11, d, fmaT(ms7, e, third * f));
+    const T quarter = cst<T>(0.25);
     T t;
-    t = a - T(4) * b + T(3) * c;
-    const T is0 = fmaT(T(0.25), t * t, q0);
+    t = fmaT(cst<T>(-4.0), b, fmaT(cst<T>(3.0), c, a));
+    const T is0 = fmaT(quarter, t * t, q0);
     t = d - b;
-    const T is1 = fmaT(T(0.25), t * t, q1);
-    t = T(-3) * c + T(4) * d - e;
-    const T is2 = fmaT(T(0.25), t * t, q2);
-    t = T(-5) * d + T(8) * e - T(3) * f;
-    T is3 = fmaT(T(0.25), t * t, q3);
-    is3 = fmax(fmax(fmax(is0, is1), is2), is3);
+    const T is1 = fmaT(quarter, t * t, q1);
+    t = fmaT(cst<T>(3.0), d - c, d - e);
+    const T is2 = fmaT(quarter, t * t, q2);
+    t = fmaT(cst<T>(8.0), e, fmaT(cst<T>(-5.0), d, cst<T>(-3.0) * f));
+    T is3 = fmaT(quarter, t * t, q3);
+    is3 = fmaxT(fmaxT(fmaxT(is0, is1), is2), is3);
     const T d0 = eps + is0, d1 = eps + is1, d2 = eps + is2, d3 = eps + is3;
     const T d01 = d0 * d1, d23 = d2 * d3;
-    const T n0 = T(0.05) * (d1 * d23);
-    const T n1 = T(0.45) * (d0 * d23);
-    const T n2 = T(0.45) * (d01 * d3);
-    const T n3 = T(0.05) * (d01 * d2);
+    const T n0 = cst<T>(0.05) * (d1 * d23);
+    const T n1 = cst<T>(0.45) * (d0 * d23);
+    const T n2 = cst<T>(0.45) * (d01 * d3);
+    const T n3 = cst<T>(0.05) * (d01 * d2);
     const T inv = rcp<T>(n0 + n1 + n2 + n3);
-    return (n0 * p0 + n1 * p1 + n2 * p2 + n3 * p3) * inv;
+    return fmaT(n0, p0, fmaT(n1, p1, fmaT(n2, p2, n3 * p3))) * inv;
 }
 
 // Both interface values of the stencil (LLL, LL, L, R, RR, RRR): wl seen from
@@ -83,12 +99,12 @@ __device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1,
 template <typename T>
 __device__ __forceinline__ void weno_pair(T LLL, T LL, T L, T R, T RR, T RRR, T eps, T &wl, T &wr)
 {
-    const T k13 = T(13) / T(12);
+    const T k13 = cst<T>(13.0 / 12.0), m2 = cst<T>(-2.0);
     T s;
-    s = LLL - T(2) * LL + L;  const T q0 = k13 * s * s;
-    s = LL - T(2) * L + R;    const T q1 = k13 * s * s;
-    s = L - T(2) * R + RR;    const T q2 = k13 * s * s;
-    s = R - T(2) * RR + RRR;  const T q3 = k13 * s * s;
+    s = fmaT(m2, LL, LLL + L);  const T q0 = k13 * s * s;
+    s = fmaT(m2, L, LL + R);    const T q1 = k13 * s * s;
+    s = fmaT(m2, R, L + RR);    const T q2 = k13 * s * s;
+    s = fmaT(m2, RR, R + RRR);  const T q3 = k13 * s * s;
     wl = weno_side<T>(LLL, LL, L, R, RR, RRR, q0, q1, q2, q3, eps);
     wr = weno_side<T>(RRR, RR, R, L, LL, LLL, q3, q2, q1, q0, eps);
 }
@@ -113,9 +129,9 @@ __device__ __forceinline__ void half_table(double U, double s, double h0, double
 {
     // h0 = 0.5 erfc(...), g = +- 0.5 exp(-lambda U^2)/sqrt(pi lambda)
     h[0] = h0;
-    h[1] = U * h0 + g;
+    h[1] = fma(U, h0, g);
 #pragma unroll
-    for (int n = 2; n < N; ++n) h[n] = U * h[n - 1] + double(n - 1) * s * h[n - 2];
+    for (int n = 2; n < N; ++n) h[n] = fma(U, h[n - 1], (double(n - 1) * s) * h[n - 2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -133,7 +149,7 @@ __device__ __forceinline__ Prim prim(const double W[5], double gm1)
     p.U0 = W[1] * p.rinv;
     p.U1 = W[2] * p.rinv;
     p.U2 = W[3] * p.rinv;
-    p.P = gm1 * (W[4] - 0.5 * (W[1] * p.U0 + W[2] * p.U1 + W[3] * p.U2));
+    p.P = gm1 * fma(-0.5, fma(W[1], p.U0, fma(W[2], p.U1, W[3] * p.U2)), W[4]);
     p.s = p.P * p.rinv;
     p.lam = 0.5 * p.den * rcp<double>(p.P);
     return p;

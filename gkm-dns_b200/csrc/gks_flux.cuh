@@ -38,28 +38,37 @@
 
 namespace gks {
 
-// Constants of one Maxwellian in its transverse co-moving frame.
+// Constants of one Maxwellian in its transverse co-moving frame.  The
+// negated copies let every use be a plain fused multiply-add, also for the
+// paired type f2, whose instructions take no operand negation.
 template <typename T> struct CoFrame {
-    T U0, U1, U2, hu2; // velocity; hu2 = (U1^2 + U2^2)/2
-    T s, tl, kal2, qn; // 1/(2 lambda), 2 lambda, kA lambda^2, U0^2 + (K+3) s
-    T r2, r4, q4;      // <rho^2>, <rho^4>, <c1^2 rho^2>
+    T U1, U2, hu2;        // transverse velocity, hu2 = (U1^2 + U2^2)/2 (to_lab)
+    T nU1, nU2, nhu2;     // their negatives (to_prime)
+    T nU0, m2U0, nqn, nqh; // -U0, -2 U0, -qn, -qn/2 with qn = U0^2 + (K+3) s (solve)
+    T tl, kal2;           // 2 lambda, kA lambda^2 (solve)
+    T s, r2, r4, q4;      // 1/(2 lambda), <rho^2>, <rho^4>, <c1^2 rho^2> (moments)
 };
 
 template <typename T>
-__device__ __forceinline__ CoFrame<T> co_frame(const Prim &g, int K, double kA)
+__device__ __forceinline__ CoFrame<T> co_frame(T U0, T U1, T U2, T s, T lam, int K, T kA)
 {
     CoFrame<T> f;
-    f.U0 = T(g.U0);
-    f.U1 = T(g.U1);
-    f.U2 = T(g.U2);
-    f.s = T(g.s);
-    const T lam = T(g.lam);
-    f.hu2 = T(0.5f) * fmaT(f.U1, f.U1, f.U2 * f.U2);
+    f.U1 = U1;
+    f.U2 = U2;
+    f.hu2 = T(0.5f) * fmaT(U1, U1, U2 * U2);
+    const T m1 = T(-1.0f);
+    f.nU1 = m1 * U1;
+    f.nU2 = m1 * U2;
+    f.nhu2 = m1 * f.hu2;
+    f.nU0 = m1 * U0;
+    f.m2U0 = T(-2.0f) * U0;
+    f.nqn = fmaT(f.nU0, U0, T(float(-(K + 3))) * s);
+    f.nqh = T(0.5f) * f.nqn;
     f.tl = T(2.0f) * lam;
-    f.kal2 = (T(kA) * lam) * lam;
-    f.qn = fmaT(f.U0, f.U0, T(float(K + 3)) * f.s);
-    f.r2 = T(float(K + 2)) * f.s;
-    const T s2 = f.s * f.s;
+    f.kal2 = (kA * lam) * lam;
+    f.s = s;
+    f.r2 = T(float(K + 2)) * s;
+    const T s2 = s * s;
     f.q4 = T(float(K + 4)) * s2;
     f.r4 = T(float((K + 2) * (K + 4))) * s2;
     return f;
@@ -67,20 +76,26 @@ __device__ __forceinline__ CoFrame<T> co_frame(const Prim &g, int K, double kA)
 
 // Primed -> lab frame of a moment vector (m = T m').
 template <typename T>
-__device__ __forceinline__ void to_lab(T m[5], T U1, T U2, T hu2)
+__device__ __forceinline__ void to_lab(T m[5], const CoFrame<T> &f)
 {
-    m[4] = fmaT(U1, m[2], fmaT(U2, m[3], fmaT(hu2, m[0], m[4])));
-    m[2] = fmaT(U1, m[0], m[2]);
-    m[3] = fmaT(U2, m[0], m[3]);
+    m[4] = fmaT(f.U1, m[2], fmaT(f.U2, m[3], fmaT(f.hu2, m[0], m[4])));
+    m[2] = fmaT(f.U1, m[0], m[2]);
+    m[3] = fmaT(f.U2, m[0], m[3]);
 }
 
 // Lab -> primed frame of a slope right-hand side (b' = T^-1 b).
 template <typename T>
-__device__ __forceinline__ void to_prime(T b[5], T U1, T U2, T hu2)
+__device__ __forceinline__ void to_prime(T b[5], T nU1, T nU2, T nhu2)
 {
-    b[2] = fmaT(-U1, b[0], b[2]);
-    b[3] = fmaT(-U2, b[0], b[3]);
-    b[4] = fmaT(-U1, b[2], fmaT(-U2, b[3], fmaT(-hu2, b[0], b[4])));
+    b[2] = fmaT(nU1, b[0], b[2]);
+    b[3] = fmaT(nU2, b[0], b[3]);
+    b[4] = fmaT(nU1, b[2], fmaT(nU2, b[3], fmaT(nhu2, b[0], b[4])));
+}
+
+template <typename T>
+__device__ __forceinline__ void to_prime(T b[5], const CoFrame<T> &f)
+{
+    to_prime<T>(b, f.nU1, f.nU2, f.nhu2);
 }
 
 // Slope solve (slopesolver, GKMflux.cpp:280-296) in the primed frame: the
@@ -90,13 +105,13 @@ __device__ __forceinline__ void to_prime(T b[5], T U1, T U2, T hu2)
 template <typename T>
 __device__ __forceinline__ void solve(const T b[5], const CoFrame<T> &f, T a[5])
 {
-    const T R2 = fmaT(-f.U0, b[0], b[1]);
-    const T R5 = fmaT(-f.qn, b[0], T(2.0f) * b[4]);
-    a[4] = f.kal2 * fmaT(T(-2.0f) * f.U0, R2, R5);
+    const T R2 = fmaT(f.nU0, b[0], b[1]);
+    const T R5 = fmaT(f.nqn, b[0], T(2.0f) * b[4]);
+    a[4] = f.kal2 * fmaT(f.m2U0, R2, R5);
     a[3] = f.tl * b[3];
     a[2] = f.tl * b[2];
-    a[1] = fmaT(-f.U0, a[4], f.tl * R2);
-    a[0] = fmaT(-f.U0, a[1], fmaT(T(-0.5f) * f.qn, a[4], b[0]));
+    a[1] = fmaT(f.nU0, a[4], f.tl * R2);
+    a[0] = fmaT(f.nU0, a[1], fmaT(f.nqh, a[4], b[0]));
 }
 
 // M = <psi' u^k (a.psi')> over the normal table X (primed frame):
@@ -119,27 +134,37 @@ __device__ __forceinline__ void mom_n(T M[5], const T *X, const CoFrame<T> &f, c
     M[4] = T(0.5f) * fmaT(c2, X[k + 2], fmaT(c0, X[k], fmaT(a[1], fmaT(f.r2, X[k + 1], X[k + 3]), h * X[k + 4])));
 }
 
-// M = <psi' u^k c_D (a.psi')>, D = 2 (c1) or 3 (c2):
-//   M0 = aD s X[k],  M1 = aD s X[k+1],  M_{5-D} = 0
+// acc += M with M = mom_n<k>(X, a), every product fused into the sum.
+template <int k, typename T>
+__device__ __forceinline__ void acc_mom_n(T acc[5], const T *X, const CoFrame<T> &f, const T a[5])
+{
+    const T h = T(0.5f) * a[4];
+    const T al = fmaT(h, f.r2, a[0]);
+    acc[0] = fmaT(al, X[k], fmaT(a[1], X[k + 1], fmaT(h, X[k + 2], acc[0])));
+    acc[1] = fmaT(al, X[k + 1], fmaT(a[1], X[k + 2], fmaT(h, X[k + 3], acc[1])));
+    const T sx = f.s * X[k];
+    acc[2] = fmaT(a[2], sx, acc[2]);
+    acc[3] = fmaT(a[3], sx, acc[3]);
+    const T c2 = fmaT(h, f.r2, al);
+    const T c0 = fmaT(a[0], f.r2, h * f.r4);
+    acc[4] = fmaT(T(0.5f), fmaT(c2, X[k + 2], fmaT(c0, X[k], fmaT(a[1], fmaT(f.r2, X[k + 1], X[k + 3]), h * X[k + 4]))),
+                  acc[4]);
+}
+
+// acc += <psi' u^k c_D (a.psi')>, D = 2 (c1) or 3 (c2); component 5 - D of
+// the moment vanishes and is skipped:
+//   M0 = aD s X[k],  M1 = aD s X[k+1]
 //   M_D = s (a0 X[k] + a1 X[k+1] + h X[k+2]) + h q4 X[k]
 //   M4 = aD (s X[k+2] + q4 X[k]) / 2
 template <int k, int D, typename T>
-__device__ __forceinline__ void mom_t(T M[5], const T *X, const CoFrame<T> &f, const T a[5])
+__device__ __forceinline__ void acc_mom_t(T acc[5], const T *X, const CoFrame<T> &f, const T a[5])
 {
     const T h = T(0.5f) * a[4];
     const T sa = f.s * a[D];
-    M[0] = sa * X[k];
-    M[1] = sa * X[k + 1];
-    M[D] = fmaT(f.s, fmaT(a[0], X[k], fmaT(a[1], X[k + 1], h * X[k + 2])), (h * f.q4) * X[k]);
-    M[5 - D] = T(0.0f);
-    M[4] = (T(0.5f) * a[D]) * fmaT(f.s, X[k + 2], f.q4 * X[k]);
-}
-
-template <typename T>
-__device__ __forceinline__ void add5(T acc[5], const T x[5])
-{
-#pragma unroll
-    for (int q = 0; q < 5; ++q) acc[q] += x[q];
+    acc[0] = fmaT(sa, X[k], acc[0]);
+    acc[1] = fmaT(sa, X[k + 1], acc[1]);
+    acc[D] = fmaT(f.s, fmaT(a[0], X[k], fmaT(a[1], X[k + 1], h * X[k + 2])), fmaT(h * f.q4, X[k], acc[D]));
+    acc[4] = fmaT(T(0.5f) * a[D], fmaT(f.s, X[k + 2], f.q4 * X[k]), acc[4]);
 }
 
 // Zeroth-order moment vectors of one Maxwellian in the lab frame, FP64:
@@ -156,17 +181,24 @@ __device__ __forceinline__ void mom0_lab(double M[5], const double *X, const Pri
     M[4] = fma(0.5, X[k + 2], c4 * X[k]);
 }
 
-// One of the two initial Maxwellians (NEG = 0: left state, half space u > 0;
-// NEG = 1: right state, u < 0).  Adds its share of W0 and of the p3 flux term
-// (double), of the transverse right-hand sides by_, bz_ of the equilibrium
-// slopes, of B_ and of the p4 / p5 flux terms (type S, lab frame).
-template <typename S, int NEG, typename Src>
-__device__ __forceinline__ void flux_side(const Src &src, const Prim &g, const FluxConst &c, double w45, double g5,
-                                          double p3, double p4, double p5, double We[5], double Fb[5], S by[5],
-                                          S bz[5], S Bs[5], S Fs[5])
+// Weights of the time integration (GKMflux.cpp:155-157, 186-190) that the
+// side passes use; the equilibrium pass forms its own from tau, ex, om, igm0.
+struct SideWeights {
+    double w45, g5, p3, p4, p5; // gm4 + gm5, gm5, p3, p4, p5
+};
+
+// Double part of the pass over one initial Maxwellian (NEG = 0: left state,
+// half space u > 0; NEG = 1: right state, u < 0): its primitive state, its
+// normal-velocity tables -- half space (GKMflux.cpp:52-60) and full space --
+// and its share of W0 (GKMflux.cpp:71-75) and of the p3 flux term
+// (GKMflux.cpp:209-212), added to the double sums of `src` (slots 0-4, 5-9).
+template <int NEG, typename Src>
+__device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, double p3, double Xh[7], double Xf[6])
 {
-    // normal-velocity tables (double): half space (GKMflux.cpp:52-60) and full space
-    double Xh[7], Xf[6];
+    constexpr bool FIRST = NEG == 0;
+    double W[5];
+    src.state(NEG, W);
+    const Prim g = prim(W, c.gm1);
     {
         const double sl = sqrt(g.lam);
         const double h0 = 0.5 * erfc(NEG ? sl * g.U0 : -sl * g.U0);
@@ -174,156 +206,247 @@ __device__ __forceinline__ void flux_side(const Src &src, const Prim &g, const F
         half_table<7>(g.U0, g.s, h0, NEG ? -ex : ex, Xh);
     }
     full_table<6, double>(g.U0, g.s, Xf);
-    // W0 (GKMflux.cpp:71-75) and the p3 term of F (GKMflux.cpp:209-212), double
-    {
-        const double c4 = fma(0.5, g.U1 * g.U1 + g.U2 * g.U2, double(c.K + 2) * 0.5 * g.s);
-        double M[5];
-        mom0_lab<0>(M, Xh, g, c4);
+    const double c4 = fma(0.5, fma(g.U1, g.U1, g.U2 * g.U2), double(c.K + 2) * 0.5 * g.s);
+    double M[5];
+    mom0_lab<0>(M, Xh, g, c4);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) We[q] = fma(g.den, M[q], We[q]);
-        mom0_lab<1>(M, Xh, g, c4);
-        const double w = p3 * g.den;
+    for (int q = 0; q < 5; ++q) src.template put_d<FIRST>(q, g.den, M[q]);
+    mom0_lab<1>(M, Xh, g, c4);
+    const double w = p3 * g.den;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Fb[q] = fma(w, M[q], Fb[q]);
-    }
-    const CoFrame<S> f = co_frame<S>(g, c.K, c.kA);
-    S Xhs[7], Xfs[6];
-#pragma unroll
-    for (int n = 0; n < 7; ++n) Xhs[n] = S(Xh[n]);
-#pragma unroll
-    for (int n = 0; n < 6; ++n) Xfs[n] = S(Xf[n]);
+    for (int q = 0; q < 5; ++q) src.template put_d<FIRST>(5 + q, w, M[q]);
+    return g;
+}
+
+// Slope part of the side pass, on the arithmetic type T of the flux assembly:
+// double (one Maxwellian), or f2 (the left and right Maxwellians as the two
+// lanes of paired FP32 instructions).  `io` supplies the slopes,
+//   io.slope(d, b)        the slope vector along d = normal, 1st, 2nd transverse
+// and takes the lab-frame results,
+//   io.emit(slot, den, M) adds den * M to S sum slot `slot` (lanes summed):
+// the transverse right-hand sides by_, bz_ of the equilibrium slopes (slots
+// 0-4, 5-9), B_ (10-14) and the p4 / p5 flux terms (15-19).
+template <typename T, typename IO>
+__device__ __forceinline__ void side_slopes(const IO &io, const CoFrame<T> &f, const T *Xh, const T *Xf, T rinv,
+                                            T den, T w45, T g5, T p4, T p5)
+{
     // slope coefficients (phase I, GKMflux.cpp:102-117) and the moment sums they
-    // feed, in the primed frame: Bp -> A (phase II, GKMflux.cpp:128-144),
+    // feed, in the primed frame: Bm = -B -> A (phase II, GKMflux.cpp:128-144),
     // Bq -> B_ (GKMflux.cpp:172-173), Fq -> F (GKMflux.cpp:210-211);
     // ayz = U1 ay + U2 az collects the v / w weights' shift.
-    S Bp[5], Bq[5], Fq[5], ayz[5];
+    T Bm[5], Bq[5], Fq[5], ayz[5];
     {
-        S DW[3][5];
-        src.slopes(NEG, DW);
-        const S rinv = S(g.rinv);
-        S a[5], b[5], M[5];
+        T a[5], b[5], M[5];
+        const T one(1.0f);
         // normal slope
+        io.slope(0, b);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] = DW[0][q] * rinv;
-        to_prime<S>(b, f.U1, f.U2, f.hu2);
-        solve<S>(b, f, a);
-        mom_n<1, S>(M, Xfs, f, a);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) Bp[q] = -M[q];
-        mom_n<1, S>(Bq, Xhs, f, a);
-        mom_n<2, S>(Fq, Xhs, f, a);
+        for (int q = 0; q < 5; ++q) b[q] *= rinv;
+        to_prime<T>(b, f);
+        solve<T>(b, f, a);
+        mom_n<1, T>(Bm, Xf, f, a);
+        mom_n<1, T>(Bq, Xh, f, a);
+        mom_n<2, T>(Fq, Xh, f, a);
         // first transverse slope (weight v = c1 + U1)
+        io.slope(1, b);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] = DW[1][q] * rinv;
-        to_prime<S>(b, f.U1, f.U2, f.hu2);
-        solve<S>(b, f, a);
-        mom_t<0, 2, S>(M, Xfs, f, a);
+        for (int q = 0; q < 5; ++q) b[q] *= rinv;
+        to_prime<T>(b, f);
+        solve<T>(b, f, a);
+        acc_mom_t<0, 2, T>(Bm, Xf, f, a);
+        mom_n<0, T>(M, Xh, f, a);
+        to_lab<T>(M, f);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Bp[q] -= M[q];
-        mom_n<0, S>(M, Xhs, f, a);
-        to_lab<S>(M, f.U1, f.U2, f.hu2);
-        add5<S>(by, M);
-        mom_t<0, 2, S>(M, Xhs, f, a);
-        add5<S>(Bq, M);
-        mom_t<1, 2, S>(M, Xhs, f, a);
-        add5<S>(Fq, M);
+        for (int q = 0; q < 5; ++q) io.emit(q, one, M[q]);
+        acc_mom_t<0, 2, T>(Bq, Xh, f, a);
+        acc_mom_t<1, 2, T>(Fq, Xh, f, a);
 #pragma unroll
         for (int q = 0; q < 5; ++q) ayz[q] = f.U1 * a[q];
         // second transverse slope (weight w = c2 + U2)
+        io.slope(2, b);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] = DW[2][q] * rinv;
-        to_prime<S>(b, f.U1, f.U2, f.hu2);
-        solve<S>(b, f, a);
-        mom_t<0, 3, S>(M, Xfs, f, a);
+        for (int q = 0; q < 5; ++q) b[q] *= rinv;
+        to_prime<T>(b, f);
+        solve<T>(b, f, a);
+        acc_mom_t<0, 3, T>(Bm, Xf, f, a);
+        mom_n<0, T>(M, Xh, f, a);
+        to_lab<T>(M, f);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Bp[q] -= M[q];
-        mom_n<0, S>(M, Xhs, f, a);
-        to_lab<S>(M, f.U1, f.U2, f.hu2);
-        add5<S>(bz, M);
-        mom_t<0, 3, S>(M, Xhs, f, a);
-        add5<S>(Bq, M);
-        mom_t<1, 3, S>(M, Xhs, f, a);
-        add5<S>(Fq, M);
+        for (int q = 0; q < 5; ++q) io.emit(5 + q, one, M[q]);
+        acc_mom_t<0, 3, T>(Bq, Xh, f, a);
+        acc_mom_t<1, 3, T>(Fq, Xh, f, a);
 #pragma unroll
         for (int q = 0; q < 5; ++q) ayz[q] = fmaT(f.U2, a[q], ayz[q]);
-        mom_n<0, S>(M, Xfs, f, ayz);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) Bp[q] -= M[q];
+        acc_mom_n<0, T>(Bm, Xf, f, ayz);
     }
-    // time-derivative coefficients of this Maxwellian (GKMflux.cpp:142-144)
-    S A[5];
-    solve<S>(Bp, f, A);
+    // time-derivative coefficients of this Maxwellian (GKMflux.cpp:142-144):
+    // An = -A from Bm = -B
+    T An[5];
+    solve<T>(Bm, f, An);
     // its B_ and F contributions (GKMflux.cpp:172-176, 209-212), lab frame
     {
-        const S sw45 = S(w45), sg5 = S(g5), sp4 = S(p4), sp5 = S(p5), den = S(g.den);
-        S cc[5], M[5];
+        T cc[5], M[5];
 #pragma unroll
-        for (int q = 0; q < 5; ++q) cc[q] = fmaT(sw45, ayz[q], sg5 * A[q]);
-        mom_n<0, S>(M, Xhs, f, cc);
+        for (int q = 0; q < 5; ++q) cc[q] = fmaT(w45, ayz[q], g5 * An[q]);
+        mom_n<0, T>(M, Xh, f, cc);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) M[q] = fmaT(sw45, Bq[q], M[q]);
-        to_lab<S>(M, f.U1, f.U2, f.hu2);
+        for (int q = 0; q < 5; ++q) M[q] = fmaT(w45, Bq[q], M[q]);
+        to_lab<T>(M, f);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Bs[q] = fmaT(den, M[q], Bs[q]);
+        for (int q = 0; q < 5; ++q) io.emit(10 + q, den, M[q]);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) cc[q] = fmaT(sp4, ayz[q], sp5 * A[q]);
-        mom_n<1, S>(M, Xhs, f, cc);
+        for (int q = 0; q < 5; ++q) cc[q] = fmaT(p4, ayz[q], p5 * An[q]);
+        mom_n<1, T>(M, Xh, f, cc);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) M[q] = fmaT(sp4, Fq[q], M[q]);
-        to_lab<S>(M, f.U1, f.U2, f.hu2);
+        for (int q = 0; q < 5; ++q) M[q] = fmaT(p4, Fq[q], M[q]);
+        to_lab<T>(M, f);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Fs[q] = fmaT(den, M[q], Fs[q]);
+        for (int q = 0; q < 5; ++q) io.emit(15 + q, den, M[q]);
     }
 }
 
+// Slope inputs and results of one side pass in double.
+template <int NEG, typename Src>
+struct SideIO64 {
+    const Src &src;
+    __device__ __forceinline__ void slope(int d, double b[5]) const { src.slope(NEG, d, b); }
+    __device__ __forceinline__ void emit(int slot, double a, double m) const
+    {
+        src.template put_s<NEG == 0>(slot, a, m);
+    }
+};
+
+// Slope inputs and results of the paired side pass (left lane .x, right .y).
+template <typename Src>
+struct SideIO2 {
+    const Src &src;
+    __device__ __forceinline__ void slope(int d, f2 b[5]) const
+    {
+        float l[5], r[5];
+        src.slope(0, d, l);
+        src.slope(1, d, r);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) b[q] = f2(l[q], r[q]);
+    }
+    __device__ __forceinline__ void emit(int slot, f2 a, f2 m) const
+    {
+        src.put_raw_s(slot, __fmaf_rn(a.v.y, m.v.y, __fmul_rn(a.v.x, m.v.x)));
+    }
+};
+
+// The two side passes of the FP64 path, one after the other; the equilibrium
+// pass reads the parked sums behind a compiler memory barrier, so that the
+// scheduler cannot start its long erfc / exp chains early and keep the side
+// passes' state live at the same time.
+template <typename Src>
+__device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, const SideWeights &tw, double)
+{
+    {
+        double Xh[7], Xf[6];
+        const Prim g = side_tables<0>(src, c, tw.p3, Xh, Xf);
+        const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.K, c.kA);
+        side_slopes<double>(SideIO64<0, Src>{src}, f, Xh, Xf, g.rinv, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
+    }
+    {
+        double Xh[7], Xf[6];
+        const Prim g = side_tables<1>(src, c, tw.p3, Xh, Xf);
+        const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.K, c.kA);
+        side_slopes<double>(SideIO64<1, Src>{src}, f, Xh, Xf, g.rinv, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
+    }
+    asm volatile("" ::: "memory");
+}
+
+// The mixed path: the double parts of the two side passes (their erfc / exp
+// chains overlap), then their FP32 slope parts together as the lanes of
+// paired instructions.
+template <typename Src>
+__device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, const SideWeights &tw, float)
+{
+    f2 Xh[7], Xf[6];
+    f2 U0, U1, U2, s, lam, rinv, den;
+    {
+        double XhL[7], XfL[6];
+        const Prim g = side_tables<0>(src, c, tw.p3, XhL, XfL);
+#pragma unroll
+        for (int n = 0; n < 7; ++n) Xh[n].v.x = float(XhL[n]);
+#pragma unroll
+        for (int n = 0; n < 6; ++n) Xf[n].v.x = float(XfL[n]);
+        U0.v.x = float(g.U0); U1.v.x = float(g.U1); U2.v.x = float(g.U2);
+        s.v.x = float(g.s); lam.v.x = float(g.lam); rinv.v.x = float(g.rinv); den.v.x = float(g.den);
+    }
+    {
+        double XhR[7], XfR[6];
+        const Prim g = side_tables<1>(src, c, tw.p3, XhR, XfR);
+#pragma unroll
+        for (int n = 0; n < 7; ++n) Xh[n].v.y = float(XhR[n]);
+#pragma unroll
+        for (int n = 0; n < 6; ++n) Xf[n].v.y = float(XfR[n]);
+        U0.v.y = float(g.U0); U1.v.y = float(g.U1); U2.v.y = float(g.U2);
+        s.v.y = float(g.s); lam.v.y = float(g.lam); rinv.v.y = float(g.rinv); den.v.y = float(g.den);
+    }
+    const CoFrame<f2> f = co_frame<f2>(U0, U1, U2, s, lam, c.K, f2(float(c.kA)));
+    side_slopes<f2>(SideIO2<Src>{src}, f, Xh, Xf, rinv, den, f2(float(tw.w45)), f2(float(-tw.g5)),
+                    f2(float(tw.p4)), f2(float(-tw.p5)));
+    asm volatile("" ::: "memory");
+}
+
+// p = (gamma - 1)(E - |m|^2 / (2 rho)), as in prim().
+__device__ __forceinline__ double pressure(const double W[5], double gm1)
+{
+    const double ri = rcp<double>(W[0]);
+    return gm1 * fma(-0.5, fma(W[1], W[1] * ri, fma(W[2], W[2] * ri, W[3] * (W[3] * ri))), W[4]);
+}
+
 // Time-integrated BGK-NS flux through one interface, in the frame of the
-// interface normal.  The caller supplies the inputs through `src`, which is
-// asked for them only when they are needed, so that one side's inputs are not
-// live while the other side is processed:
-//   src.state(side, W)      reconstructed state Wl (side 0) or Wr (side 1)
-//   src.slopes(side, DW)    its slopes DW[d][q], d = normal, 1st, 2nd transverse
-//   src.cells(WL, WR)       the cell averages either side of the interface
+// interface normal.  `src` supplies the inputs when they are needed, so that
+// one side's inputs are not live while the other side is processed, and keeps
+// the running sums of the two side passes:
+//   src.state(side, W)        reconstructed state Wl (side 0) or Wr (side 1)
+//   src.slope(side, d, DW)    its slopes along d = normal, 1st, 2nd transverse
+//   src.cells(WL, WR)         the cell averages either side of the interface
+//   src.put_d / put_s<FIRST>(slot, v), get_d / get_s(slot)   running sums
 // tau0 = mu/p at the left cell.  Output F[5], the flux integrated over [0, dt].
 template <typename S, typename Src>
 __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const FluxConst &c, double F[5])
 {
-    Prim l, r;
-    {
-        double Ws[5];
-        src.state(0, Ws);
-        l = prim(Ws, c.gm1);
-        src.state(1, Ws);
-        r = prim(Ws, c.gm1);
-    }
-    // collision time with the pressure-jump term (GKMflux.cpp:149-150):
-    // rho/lambda = 2p, so w = |p_l - p_r| / (p_l + p_r)
     const double dt = c.dt;
-    const double tau = tau0 + dt * (fabs(l.P - r.P) * rcp<double>(l.P + r.P));
-    const double ex = exp(-dt * rcp<double>(tau));
-    const double om = 1.0 - ex;
-    // gamma weights (GKMflux.cpp:155-157)
-    const double igm0 = rcp<double>(dt - tau * om);
-    const double gm1 = -om * igm0;
-    const double gm2 = (-dt + 2.0 * tau * om - dt * ex) * igm0;
-    const double gm3 = -gm1;
-    const double gm4 = (dt * ex - tau * om) * igm0;
-    const double gm5 = tau * gm3;
-    // time integrals (GKMflux.cpp:186-190)
-    const double Pt = tau * om;
-    const double Qt = tau * (tau * om - dt * ex);
+    double tau, ex, om, igm0;
+    SideWeights tw;
+    {
+        // collision time with the pressure-jump term (GKMflux.cpp:149-150):
+        // rho/lambda = 2p, so w = |p_l - p_r| / (p_l + p_r)
+        double W[5];
+        src.state(0, W);
+        const double pl = pressure(W, c.gm1);
+        src.state(1, W);
+        const double pr = pressure(W, c.gm1);
+        tau = fma(dt, fabs(pl - pr) * rcp<double>(pl + pr), tau0);
+        ex = exp(-dt * rcp<double>(tau));
+        om = 1.0 - ex;
+        // gamma weights (GKMflux.cpp:155-157) and time integrals (GKMflux.cpp:186-190)
+        const double Pt = tau * om;
+        igm0 = rcp<double>(dt - Pt);
+        const double gm3 = om * igm0;
+        const double gm4 = fma(dt, ex, -Pt) * igm0;
+        tw.g5 = tau * gm3;
+        tw.w45 = gm4 + tw.g5;
+        const double Qt = tau * fma(-dt, ex, Pt);
+        tw.p3 = Pt;
+        tw.p4 = fma(-tau, Pt, -Qt);
+        tw.p5 = -tau * Pt;
+    }
+    flux_sides(src, c, tw, S());
+    const double gm1 = -om * igm0, gm3 = -gm1;
+    const double Pt = tau * om, Qt = tau * fma(-dt, ex, Pt);
+    const double gm2 = fma(-dt, ex, fma(2.0, Pt, -dt)) * igm0;
     const double p0 = dt - Pt;
-    const double p1 = 0.5 * dt * dt - tau * p0;
-    const double p2 = -tau * p0 + Qt;
-    const double p3 = Pt;
-    const double p4 = -Qt - tau * Pt;
-    const double p5 = -tau * Pt;
-
-    double We[5] = {0, 0, 0, 0, 0}, Fb[5] = {0, 0, 0, 0, 0};
-    S by[5] = {0, 0, 0, 0, 0}, bz[5] = {0, 0, 0, 0, 0}, Bs[5] = {0, 0, 0, 0, 0}, Fs[5] = {0, 0, 0, 0, 0};
-    flux_side<S, 0>(src, l, c, gm4 + gm5, gm5, p3, p4, p5, We, Fb, by, bz, Bs, Fs);
-    flux_side<S, 1>(src, r, c, gm4 + gm5, gm5, p3, p4, p5, We, Fb, by, bz, Bs, Fs);
+    const double p1 = fma(0.5 * dt, dt, -tau * p0);
+    const double p2 = fma(-tau, p0, Qt);
 
     // equilibrium state at the interface and its tables (GKMflux.cpp:75-98)
+    double We[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) We[q] = src.get_d(q);
     const Prim e = prim(We, c.gm1);
     double Xf[6], Xp[7], Xn[7];
     full_table<6, double>(e.U0, e.s, Xf);
@@ -337,24 +460,20 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         half_table<7>(e.U0, e.s, x >= 0.0 ? 1.0 - tail : tail, g, Xp);
         half_table<7>(e.U0, e.s, x >= 0.0 ? tail : 1.0 - tail, -g, Xn);
     }
+    const double c4 = fma(0.5, fma(e.U1, e.U1, e.U2 * e.U2), double(c.K + 2) * 0.5 * e.s);
     // B_ / rho_e in the primed frame of the equilibrium, with its nearly
     // cancelling zeroth-order part gm1 rho_e <psi>_e + gm3 W0 in double
-    // (GKMflux.cpp:174-178); p0 term of F (GKMflux.cpp:209)
+    // (GKMflux.cpp:174-178)
     double Bd[5];
     {
-        const double c4 = fma(0.5, e.U1 * e.U1 + e.U2 * e.U2, double(c.K + 2) * 0.5 * e.s);
         double M[5];
         mom0_lab<0>(M, Xf, e, c4);
         const double w = gm1 * e.den;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Bd[q] = (fma(w, M[q], gm3 * We[q]) + double(Bs[q])) * e.rinv;
-        to_prime<double>(Bd, e.U1, e.U2, 0.5 * fma(e.U1, e.U1, e.U2 * e.U2));
-        mom0_lab<1>(M, Xf, e, c4);
-        const double w0 = p0 * e.den;
-#pragma unroll
-        for (int q = 0; q < 5; ++q) Fb[q] = fma(w0, M[q], Fb[q]);
+        for (int q = 0; q < 5; ++q) Bd[q] = (fma(w, M[q], gm3 * We[q]) + double(src.get_s(10 + q))) * e.rinv;
+        to_prime<double>(Bd, -e.U1, -e.U2, -0.5 * fma(e.U1, e.U1, e.U2 * e.U2));
     }
-    const CoFrame<S> f = co_frame<S>(e, c.K, c.kA);
+    const CoFrame<S> f = co_frame<S>(S(e.U0), S(e.U1), S(e.U2), S(e.s), S(e.lam), c.K, S(c.kA));
     S Xfs[6], Xps[7], Xns[7];
 #pragma unroll
     for (int n = 0; n < 6; ++n) Xfs[n] = S(Xf[n]);
@@ -364,6 +483,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         Xns[n] = S(Xn[n]);
     }
     // slopes of the equilibrium (GKMflux.cpp:109-117, 136-137)
+    asm volatile("" ::: "memory"); // parked cell averages and sums are read from here on
     S axl[5], axr[5], ay[5], az[5], ayz[5];
     {
         double WL[5], WR[5];
@@ -372,32 +492,32 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         S b[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) b[q] = S(We[q] - WL[q]) * k2;
-        to_prime<S>(b, f.U1, f.U2, f.hu2);
+        to_prime<S>(b, f);
         solve<S>(b, f, axl);
 #pragma unroll
         for (int q = 0; q < 5; ++q) b[q] = S(WR[q] - We[q]) * k2;
-        to_prime<S>(b, f.U1, f.U2, f.hu2);
+        to_prime<S>(b, f);
         solve<S>(b, f, axr);
-        to_prime<S>(by, f.U1, f.U2, f.hu2);
-        solve<S>(by, f, ay);
-        to_prime<S>(bz, f.U1, f.U2, f.hu2);
-        solve<S>(bz, f, az);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) b[q] = src.get_s(q);
+        to_prime<S>(b, f);
+        solve<S>(b, f, ay);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) b[q] = src.get_s(5 + q);
+        to_prime<S>(b, f);
+        solve<S>(b, f, az);
 #pragma unroll
         for (int q = 0; q < 5; ++q) ayz[q] = fmaT(f.U1, ay[q], f.U2 * az[q]);
     }
     // A_ (phase III, GKMflux.cpp:159-180)
     S A[5];
     {
-        S T1[5], M[5];
+        S T1[5];
         mom_n<1, S>(T1, Xps, f, axl);
-        mom_n<1, S>(M, Xns, f, axr);
-        add5<S>(T1, M);
-        mom_t<0, 2, S>(M, Xfs, f, ay);
-        add5<S>(T1, M);
-        mom_t<0, 3, S>(M, Xfs, f, az);
-        add5<S>(T1, M);
-        mom_n<0, S>(M, Xfs, f, ayz);
-        add5<S>(T1, M);
+        acc_mom_n<1, S>(T1, Xns, f, axr);
+        acc_mom_t<0, 2, S>(T1, Xfs, f, ay);
+        acc_mom_t<0, 3, S>(T1, Xfs, f, az);
+        acc_mom_n<0, S>(T1, Xfs, f, ayz);
         const S g2 = S(gm2);
         S B[5];
 #pragma unroll
@@ -409,21 +529,23 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         const S sp1 = S(p1), sp2 = S(p2);
         S T1[5], M[5], cc[5];
         mom_n<2, S>(T1, Xps, f, axl);
-        mom_n<2, S>(M, Xns, f, axr);
-        add5<S>(T1, M);
-        mom_t<1, 2, S>(M, Xfs, f, ay);
-        add5<S>(T1, M);
-        mom_t<1, 3, S>(M, Xfs, f, az);
-        add5<S>(T1, M);
+        acc_mom_n<2, S>(T1, Xns, f, axr);
+        acc_mom_t<1, 2, S>(T1, Xfs, f, ay);
+        acc_mom_t<1, 3, S>(T1, Xfs, f, az);
 #pragma unroll
         for (int q = 0; q < 5; ++q) cc[q] = fmaT(sp1, A[q], sp2 * ayz[q]);
         mom_n<1, S>(M, Xfs, f, cc);
 #pragma unroll
         for (int q = 0; q < 5; ++q) T1[q] = fmaT(sp2, T1[q], M[q]);
-        to_lab<S>(T1, f.U1, f.U2, f.hu2);
+        to_lab<S>(T1, f);
         const S dens = S(e.den);
+        asm volatile("" ::: "memory"); // the parked flux sums are read from here on
+        double M0[5];
+        mom0_lab<1>(M0, Xf, e, c4);
+        const double w0 = p0 * e.den;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) F[q] = Fb[q] + double(fmaT(dens, T1[q], Fs[q]));
+        for (int q = 0; q < 5; ++q)
+            F[q] = fma(w0, M0[q], src.get_d(5 + q)) + double(fmaT(dens, T1[q], src.get_s(15 + q)));
     }
 }
 

@@ -88,7 +88,16 @@ __device__ __forceinline__ double temperature(const double W[5], double cT)
 {
     // (gam-1)(E/rho - |m|^2/(2 rho^2))/R, update.cpp:560
     const double ri = __drcp_rn(W[0]);
-    return cT * (W[4] * ri - 0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * (ri * ri));
+    const double ke = fma(W[1], W[1], fma(W[2], W[2], W[3] * W[3]));
+    return cT * fma(-0.5 * ke, ri * ri, W[4] * ri);
+}
+
+// rho E from the reconstructed density, momentum and temperature
+// (update.cpp:618-619): rho T R/(gam-1) + |m|^2 / (2 rho), ri = 1/rho.
+__device__ __forceinline__ double energy(const double w[5], double T, double ri, double icT)
+{
+    const double ke = fma(w[1], w[1], fma(w[2], w[2], w[3] * w[3]));
+    return fma(w[0] * T, icT, (0.5 * ke) * ri);
 }
 
 // ---------------------------------------------------------------------------
@@ -96,7 +105,7 @@ __device__ __forceinline__ double temperature(const double W[5], double cT)
 // neighbour along DIR (update.cpp:247 / GPUupdate.cu:917-977).
 // ---------------------------------------------------------------------------
 template <int DIR, int PREC, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_recon(Batch b)
+__global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
@@ -127,23 +136,35 @@ __global__ void __launch_bounds__(128, MINB) k_recon(Batch b)
                 weno_pair<double>(T[0], T[1], T[2], T[3], T[4], T[5], kWenoEps, tl, tr);
                 // E from the reconstructed temperature (update.cpp:618-619)
                 const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
-                wl[4] = wl[0] * tl * f.icT + 0.5 * (wl[1] * wl[1] + wl[2] * wl[2] + wl[3] * wl[3]) * il;
-                wr[4] = wr[0] * tr * f.icT + 0.5 * (wr[1] * wr[1] + wr[2] * wr[2] + wr[3] * wr[3]) * ir;
+                wl[4] = energy(wl, tl, il, f.icT);
+                wr[4] = energy(wr, tr, ir, f.icT);
             }
         } else {
-            // mixed: WENO in FP32 on differences from the left cell, added back in FP64
+            // mixed: WENO in FP32 on differences from the left cell, added back
+            // in FP64; components (0, 1) and (2, 3) as the two lanes of paired
+            // FP32 instructions, the fifth (energy or temperature) alone
             const float epsf = float(kWenoEps);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                if (q == 4 && !direct) break;
-                const double c0 = s[2][q];
-                float dl, dr;
-                weno_pair<float>(float(s[0][q] - c0), float(s[1][q] - c0), 0.0f, float(s[3][q] - c0),
-                                 float(s[4][q] - c0), float(s[5][q] - c0), epsf, dl, dr);
-                wl[q] = c0 + double(dl);
-                wr[q] = c0 + double(dr);
+            for (int q = 0; q < 4; q += 2) {
+                const double c0 = s[2][q], c1 = s[2][q + 1];
+                f2 v[6];
+#pragma unroll
+                for (int a = 0; a < 6; ++a) v[a] = f2(float(s[a][q] - c0), float(s[a][q + 1] - c1));
+                f2 dl, dr;
+                weno_pair<f2>(v[0], v[1], f2(0.0f), v[3], v[4], v[5], f2(epsf), dl, dr);
+                wl[q] = c0 + double(dl.v.x);
+                wr[q] = c0 + double(dr.v.x);
+                wl[q + 1] = c1 + double(dl.v.y);
+                wr[q + 1] = c1 + double(dr.v.y);
             }
-            if (!direct) {
+            if (direct) {
+                const double c0 = s[2][4];
+                float dl, dr;
+                weno_pair<float>(float(s[0][4] - c0), float(s[1][4] - c0), 0.0f, float(s[3][4] - c0),
+                                 float(s[4][4] - c0), float(s[5][4] - c0), epsf, dl, dr);
+                wl[4] = c0 + double(dl);
+                wr[4] = c0 + double(dr);
+            } else {
                 double T[6];
 #pragma unroll
                 for (int a = 0; a < 6; ++a) T[a] = temperature(s[a], f.cT);
@@ -152,8 +173,8 @@ __global__ void __launch_bounds__(128, MINB) k_recon(Batch b)
                                  float(T[4] - T[2]), float(T[5] - T[2]), epsf, dl, dr);
                 const double tl = T[2] + double(dl), tr = T[2] + double(dr);
                 const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
-                wl[4] = wl[0] * tl * f.icT + 0.5 * (wl[1] * wl[1] + wl[2] * wl[2] + wl[3] * wl[3]) * il;
-                wr[4] = wr[0] * tr * f.icT + 0.5 * (wr[1] * wr[1] + wr[2] * wr[2] + wr[3] * wr[3]) * ir;
+                wl[4] = energy(wl, tl, il, f.icT);
+                wr[4] = energy(wr, tr, ir, f.icT);
             }
         }
 #pragma unroll
@@ -193,21 +214,22 @@ __device__ __forceinline__ void transverse(const Cell &x, int flags, unsigned &n
     }
 }
 
-// Inputs of one interface (see gks_flux).  All global loads are issued at
-// once when the interface starts, so that their latency overlaps; what is not
-// needed until later -- the right state's slopes and the two cell averages --
-// is parked in this thread's own shared-memory slots ([slot][thread], no bank
-// conflicts) instead of registers.  Slot q of the rotated frame holds
-// original component perm(q): rho v (y sweep) or rho w (z sweep) moves into
-// slot 1 (update.cpp:340-350, 429-439).
-constexpr int kFluxBlock = 128;
-
+// Inputs and running sums of one interface (see gks_flux).  All global loads
+// are issued at once when the interface starts, so that their latency
+// overlaps; what is not needed until later -- the right state and its slopes,
+// the two cell averages -- is parked in this thread's own shared-memory slots
+// ([slot][thread], no bank conflicts) instead of registers, and so are the
+// sums the two side passes of the flux accumulate for the equilibrium pass.
+// Slot q of the rotated frame holds original component perm(q): rho v (y
+// sweep) or rho w (z sweep) moves into slot 1 (update.cpp:340-350, 429-439).
 template <int DIR, typename S>
 struct SweepSrc {
-    double Wl[5], Wr[5];
+    double Wl[5];
     S DWl[3][5];
     S (*park_dw)[kFluxBlock];      // [15][block]: right-side slopes
-    double (*park_w)[kFluxBlock];  // [10][block]: WL, WR
+    double (*park_w)[kFluxBlock];  // [15][block]: WL, WR, Wr
+    double (*sum_d)[kFluxBlock];   // [10][block]: double sums of the side passes
+    S (*sum_s)[kFluxBlock];        // [20][block]: S sums of the side passes
 
     __device__ static constexpr int perm(int q)
     {
@@ -227,32 +249,31 @@ struct SweepSrc {
             const int o = perm(q);
             const double *rl = f.rec[o], *rr = f.rec[5 + o];
             const double wL = __ldg(f.W[o] + c), wR = __ldg(f.W[o] + c1);
+            const double wr = __ldg(rr + c);
             Wl[q] = __ldg(rl + c);
-            Wr[q] = __ldg(rr + c);
             DWl[0][q] = kn * S(Wl[q] - wL);
             DWl[1][q] = ky * S(__ldg(rl + cn) - __ldg(rl + cs));
             DWl[2][q] = kt * S(__ldg(rl + cf) - __ldg(rl + cb));
-            park_dw[q][t] = kn * S(wR - Wr[q]);
+            park_dw[q][t] = kn * S(wR - wr);
             park_dw[5 + q][t] = ky * S(__ldg(rr + cn) - __ldg(rr + cs));
             park_dw[10 + q][t] = kt * S(__ldg(rr + cf) - __ldg(rr + cb));
             park_w[q][t] = wL;
             park_w[5 + q][t] = wR;
+            park_w[10 + q][t] = wr;
         }
     }
 
     __device__ __forceinline__ void state(int side, double W[5]) const
     {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) W[q] = side == 0 ? Wl[q] : Wr[q];
+        for (int q = 0; q < 5; ++q) W[q] = side == 0 ? Wl[q] : park_w[10 + q][threadIdx.x];
     }
 
-    __device__ __forceinline__ void slopes(int side, S DW[3][5]) const
+    // slopes of one side along one direction (0 normal, 1 and 2 transverse)
+    __device__ __forceinline__ void slope(int side, int d, S DW[5]) const
     {
-        const int t = threadIdx.x;
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-            for (int q = 0; q < 5; ++q) DW[d][q] = side == 0 ? DWl[d][q] : park_dw[5 * d + q][t];
+        for (int q = 0; q < 5; ++q) DW[q] = side == 0 ? DWl[d][q] : park_dw[5 * d + q][threadIdx.x];
     }
 
     __device__ __forceinline__ void cells(double WL[5], double WR[5]) const
@@ -264,6 +285,24 @@ struct SweepSrc {
             WR[q] = park_w[5 + q][t];
         }
     }
+
+    // running sums of a * b: the first side pass stores, the second adds (one
+    // explicit rounding each, so that no compiler contraction choice -- which
+    // may differ between register-cap variants -- changes the result)
+    template <bool FIRST> __device__ __forceinline__ void put_d(int i, double a, double b) const
+    {
+        double &x = sum_d[i][threadIdx.x];
+        x = FIRST ? __dmul_rn(a, b) : __fma_rn(a, b, x);
+    }
+    template <bool FIRST> __device__ __forceinline__ void put_s(int i, S a, S b) const
+    {
+        S &x = sum_s[i][threadIdx.x];
+        if constexpr (sizeof(S) == 8) x = FIRST ? __dmul_rn(a, b) : __fma_rn(a, b, x);
+        else x = FIRST ? __fmul_rn(a, b) : __fmaf_rn(a, b, x);
+    }
+    __device__ __forceinline__ void put_raw_s(int i, S v) const { sum_s[i][threadIdx.x] = v; }
+    __device__ __forceinline__ double get_d(int i) const { return sum_d[i][threadIdx.x]; }
+    __device__ __forceinline__ S get_s(int i) const { return sum_s[i][threadIdx.x]; }
 };
 
 template <int DIR, int PREC, int MINB>
@@ -271,7 +310,9 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
 {
     using S = typename std::conditional<PREC == 0, double, float>::type;
     __shared__ S park_dw[15][kFluxBlock];
-    __shared__ double park_w[10][kFluxBlock];
+    __shared__ double park_w[15][kFluxBlock];
+    __shared__ double sum_d[10][kFluxBlock];
+    __shared__ S sum_s[20][kFluxBlock];
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
@@ -282,6 +323,8 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
         SweepSrc<DIR, S> src;
         src.park_dw = park_dw;
         src.park_w = park_w;
+        src.sum_d = sum_d;
+        src.sum_s = sum_s;
         src.load(f, x.c, along<DIR>(x, 1), cn, cs, cf, cb);
         // collision time at the left cell, in the unrotated frame (update.cpp:262-264)
         double tau0;
@@ -292,7 +335,7 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
 #pragma unroll
             for (int q = 0; q < 5; ++q) w[SweepSrc<DIR, S>::perm(q)] = WL[q];
             const double ri = __drcp_rn(w[0]);
-            const double P = f.gm1 * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) * ri);
+            const double P = f.gm1 * fma(-0.5 * fma(w[1], w[1], fma(w[2], w[2], w[3] * w[3])), ri, w[4]);
             const double T = P * ri * (1.0 / f.R);
             tau0 = viscosity(f, T) * __drcp_rn(P);
         }
@@ -320,7 +363,7 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
 // reference's order: W - (1/dx)*(Fx - Fx[i-1] + Fy - Fy[j-1] + Fz - Fz[k-1]).
 // Also flags non-finite or non-positive density / pressure.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_update(Batch b)
+__global__ void __launch_bounds__(kUpdateBlock) k_update(Batch b)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
@@ -689,16 +732,19 @@ cudaError_t occ(KernelT k, int block, int *n)
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k, block, 0);
 }
 
-// Register-cap variants (min resident blocks of 128 threads per SM); the
-// tuner picks one per kernel, precision and sweep.
-constexpr int kReconMinb[kReconVariants] = {4, 6};
-constexpr int kFluxMinb[kFluxVariants] = {1, 3, 4};
+// Register-cap variants (min resident blocks per SM: reconstruction blocks of
+// 128 threads at 3 / 4 / 6 -> 168 / 128 / 80 registers, flux blocks of 64 threads at
+// 4 / 6 / 8 -> 255 / 168 / 128 registers); the tuner picks one per
+// kernel, precision and sweep.  Every variant gives bit-identical results.
+constexpr int kReconMinb[kReconVariants] = {3, 4, 6};
+constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
 
 template <int DIR, int PREC>
 cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
 {
     switch (cfg.variant) {
     case 1: k_recon<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    case 2: k_recon<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
     default: k_recon<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
     }
     return cudaGetLastError();
@@ -720,6 +766,7 @@ cudaError_t occ_kind(int kind, int variant, int block, int *n)
 {
     if (kind == K_RECON) {
         if (variant == 1) return occ(k_recon<DIR, PREC, kReconMinb[1]>, block, n);
+        if (variant == 2) return occ(k_recon<DIR, PREC, kReconMinb[2]>, block, n);
         return occ(k_recon<DIR, PREC, kReconMinb[0]>, block, n);
     }
     if (variant == 1) return occ(k_flux<DIR, PREC, kFluxMinb[1]>, block, n);

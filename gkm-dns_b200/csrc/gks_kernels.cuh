@@ -55,8 +55,13 @@ struct LaunchCfg {
 };
 
 enum KernelKind { K_RECON = 0, K_FLUX = 1, K_UPDATE = 2, K_KINDS = 3 };
-constexpr int kReconVariants = 2;
+constexpr int kReconVariants = 3;
 constexpr int kFluxVariants = 3;
+
+// Threads per block of each kernel kind.
+constexpr int kReconBlock = 128;
+constexpr int kFluxBlock = 64;
+constexpr int kUpdateBlock = 256;
 
 // Stage launchers (asynchronous on `st`).  prec: 0 FP64, 1 mixed.
 cudaError_t launch_recon(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);

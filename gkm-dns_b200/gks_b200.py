@@ -89,6 +89,7 @@ SIGNATURES = {
     "gks_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "gks_get_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "gks_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gks_timestep_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_void_p, DP]),
 }
@@ -259,6 +260,12 @@ class Solver:
                 self._ck(self._lib.gks_get_launch(self._h, kind, d, ctypes.byref(b), ctypes.byref(g), ctypes.byref(v)))
                 out[f"{kname}_{dname}"] = {"block": b.value, "grid": g.value, "variant": v.value}
         return out
+
+    def set_launch(self, kind: str, d: int, variant: int, grid: int = 0):
+        """Pin kernel `kind` ("recon", "flux", "update") of sweep d (0, 1, 2) to a
+        register-cap variant and grid (0: one wave of resident blocks)."""
+        k = ("recon", "flux", "update").index(kind)
+        self._ck(self._lib.gks_set_launch(self._h, k, d, grid, variant))
 
     def set_stream(self, stream: int | None):
         self._ck(self._lib.gks_set_stream(self._h, ctypes.c_void_p(stream or 0)))

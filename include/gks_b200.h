@@ -157,6 +157,13 @@ int gks_autotune(gks_ctx *ctx, int reps);
  * dir 0..2 = x, y, z. */
 int gks_get_launch(gks_ctx *ctx, int kind, int dir, int *block, int *grid, int *variant);
 
+/* Pin the launch configuration of one kernel kind and sweep (for example to
+ * restore a tuning saved by a previous run): `variant` indexes the kind's
+ * register-cap variants (gks_get_launch reports the one in use), `grid` is the
+ * number of blocks of the persistent grid-stride launch, 0 for one wave of
+ * resident blocks.  Results do not depend on the configuration. */
+int gks_set_launch(gks_ctx *ctx, int kind, int dir, int grid, int variant);
+
 /* Peak FMA throughput of the FP64 (GKS_FP64) or FP32 (GKS_MIXED) pipe of
  * the current device in TFLOP/s, 2 flops per FMA (a short microbenchmark). */
 int gks_peak_flops(int precision, double *tflops);

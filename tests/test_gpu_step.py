@@ -285,6 +285,36 @@ def test_autotuned_launches_give_identical_results(gks):
         assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_every_kernel_variant_gives_identical_results(gks, prec):
+    """Each register-cap variant of the reconstruction and flux kernels, and a
+    one-block grid-stride launch, reproduce the default launch bit for bit."""
+    case = gks_ic.make_dhit(24, k0=4.0, Mt=0.5, seed=8)
+    W = gks_ic.to_conservative_padded(case)
+    p = gks.FP64 if prec == "fp64" else gks.MIXED
+
+    def run(pin):
+        with gks.Solver(gks.phys_from_case(case), p) as s:
+            s.upload(W)
+            s.timestep(0.5)
+            for kind, variant, grid in pin:
+                for d in range(3):
+                    s.set_launch(kind, d, variant, grid)
+            s.step(3)
+            s.sync()
+            return s.download()
+
+    base = run([])
+    for kind, nvar in (("recon", 3), ("flux", 3)):
+        for v in range(nvar):
+            for grid in (0, 1):
+                got = run([(kind, v, grid)])
+                diff = np.abs(got - base).max()
+                assert diff == 0.0, (prec, kind, v, grid, diff)
+    with pytest.raises(gks.GksError):
+        run([("flux", 3, 0)])
+
+
 def test_mixed_tracks_fp64(gks):
     case = gks_ic.make_dhit(32, k0=4.0, Mt=0.5, Re_lambda=100.0, seed=0)
     W = gks_ic.to_conservative_padded(case)
