@@ -156,13 +156,13 @@ gks::LaunchCfg persistent(gks_ctx *ctx, int kind, int dir, int variant, int mult
     return c;
 }
 
-// Untuned defaults: the mixed flux at the 168-register cap (its spill is
-// negligible there), everything else uncapped.
+// Untuned defaults: the flux at the 168-register cap (6 blocks of 64
+// threads per SM), the reconstruction at its natural register count.
 void choose_launch(gks_ctx *ctx)
 {
     for (int kind = 0; kind < gks::K_KINDS; ++kind)
         for (int dir = 0; dir < 3; ++dir) {
-            const int variant = (kind == gks::K_FLUX && ctx->precision == GKS_MIXED) ? 1 : 0;
+            const int variant = kind == gks::K_FLUX ? 1 : 0;
             ctx->cfg[kind][dir] = persistent(ctx, kind, dir, variant, 1);
         }
 }
