@@ -149,7 +149,8 @@ gks::LaunchCfg persistent(gks_ctx *ctx, int kind, int dir, int variant, int mult
     if (gks::max_resident_blocks(kind, dir, ctx->precision, variant, c.block, &per_sm) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     long long g = (long long)ctx->nsm * per_sm * mult;
-    const long long need = (ctx->batch.total + c.block - 1) / c.block;
+    const long long items = (kind == gks::K_RECON && dir < 2) ? ctx->batch.wtotal : ctx->batch.total;
+    const long long need = (items + c.block - 1) / c.block;
     if (g > need) g = need;
     if (g < 1) g = 1;
     c.grid = (int)g;
@@ -244,7 +245,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     ctx->own_stream = true;
 
     ctx->fh.resize(nfields);
-    long long base = 0;
+    long long base = 0, wbase = 0;
     const double pi = std::atan(1.0) * 4.0; // param.h:14
     for (int f = 0; f < nfields; ++f) {
         FieldHost &h = ctx->fh[f];
@@ -269,6 +270,11 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.base = base;
         d.ncell = n;
         base += (n + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
+        const int run = gks::win_run(precision == GKS_MIXED ? 1 : 0);
+        d.nrun = (p.nc + run - 1) / run;
+        d.nwin = (long long)p.nc * p.nc * d.nrun;
+        d.wbase = wbase;
+        wbase += (d.nwin + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
         d.nc = p.nc;
         // magic number for x / nc (round-up method): l = ceil(log2 nc),
         // m = floor(2^32 (2^l - nc) / nc) + 1, x / nc = (umulhi(x, m) + x) >> l
@@ -310,6 +316,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     ctx->batch.fields = ctx->d_fields;
     ctx->batch.nfields = nfields;
     ctx->batch.total = base;
+    ctx->batch.wtotal = wbase;
     ctx->batch.err = ctx->d_err;
     choose_launch(ctx);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(GKS_ECUDA);

@@ -7,7 +7,7 @@
 // persistent grid-stride loops over the cells of all fields, so one launch
 // covers an ensemble of fields of different sizes.  The periodic halo of the
 // reference (HaloTransfer on one rank, update.cpp:894-1054) is the index wrap
-// in `shift`.
+// in `along` and in the windowed reconstruction's cell map.
 #include "gks_device.cuh"
 #include "gks_flux.cuh"
 #include "gks_kernels.cuh"
@@ -58,13 +58,6 @@ __device__ __forceinline__ Cell decode(unsigned c, const FieldDev &f)
 
 __device__ __forceinline__ int wrap(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 
-// Linear index of the cell displaced by (dj, di, dk), periodic.
-__device__ __forceinline__ unsigned shift(const Cell &x, int dj, int di, int dk)
-{
-    const unsigned n = x.nc;
-    return ((unsigned)wrap(x.j + dj, x.nc) * n + (unsigned)wrap(x.i + di, x.nc)) * n + (unsigned)wrap(x.k + dk, x.nc);
-}
-
 // Displacement along the sweep axis: DIR 0 = x (i), 1 = y (j), 2 = z (k);
 // only the swept coordinate wraps.
 template <int DIR>
@@ -101,8 +94,70 @@ __device__ __forceinline__ double energy(const double w[5], double T, double ri,
 }
 
 // ---------------------------------------------------------------------------
+// WENO of one interface from its 6-cell stencil s[0..5] (LLL .. RRR) and the
+// stencil's temperatures T[0..5] (used unless GKS_DIRECT_ENERGY)
+// (update.cpp:247, 502-625 / GPUupdate.cu:917-977).
+// ---------------------------------------------------------------------------
+template <int PREC>
+__device__ __forceinline__ void recon_point(const double (&s)[6][5], const double (&T)[6], bool direct, double icT,
+                                            double wl[5], double wr[5])
+{
+    if (PREC == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            weno_pair<double>(s[0][q], s[1][q], s[2][q], s[3][q], s[4][q], s[5][q], kWenoEps, wl[q], wr[q]);
+        if (direct) {
+            weno_pair<double>(s[0][4], s[1][4], s[2][4], s[3][4], s[4][4], s[5][4], kWenoEps, wl[4], wr[4]);
+        } else {
+            double tl, tr;
+            weno_pair<double>(T[0], T[1], T[2], T[3], T[4], T[5], kWenoEps, tl, tr);
+            // E from the reconstructed temperature (update.cpp:618-619)
+            const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
+            wl[4] = energy(wl, tl, il, icT);
+            wr[4] = energy(wr, tr, ir, icT);
+        }
+    } else {
+        // mixed: WENO in FP32 on differences from the left cell, added back
+        // in FP64; components (0, 1) and (2, 3) as the two lanes of paired
+        // FP32 instructions, the fifth (energy or temperature) alone
+        const float epsf = float(kWenoEps);
+#pragma unroll
+        for (int q = 0; q < 4; q += 2) {
+            const double c0 = s[2][q], c1 = s[2][q + 1];
+            f2 v[6];
+#pragma unroll
+            for (int a = 0; a < 6; ++a) v[a] = f2(float(s[a][q] - c0), float(s[a][q + 1] - c1));
+            f2 dl, dr;
+            weno_pair<f2>(v[0], v[1], f2(0.0f), v[3], v[4], v[5], f2(epsf), dl, dr);
+            wl[q] = c0 + double(dl.v.x);
+            wr[q] = c0 + double(dr.v.x);
+            wl[q + 1] = c1 + double(dl.v.y);
+            wr[q + 1] = c1 + double(dr.v.y);
+        }
+        if (direct) {
+            const double c0 = s[2][4];
+            float dl, dr;
+            weno_pair<float>(float(s[0][4] - c0), float(s[1][4] - c0), 0.0f, float(s[3][4] - c0),
+                             float(s[4][4] - c0), float(s[5][4] - c0), epsf, dl, dr);
+            wl[4] = c0 + double(dl);
+            wr[4] = c0 + double(dr);
+        } else {
+            float dl, dr;
+            weno_pair<float>(float(T[0] - T[2]), float(T[1] - T[2]), 0.0f, float(T[3] - T[2]),
+                             float(T[4] - T[2]), float(T[5] - T[2]), epsf, dl, dr);
+            const double tl = T[2] + double(dl), tr = T[2] + double(dr);
+            const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
+            wl[4] = energy(wl, tl, il, icT);
+            wr[4] = energy(wr, tr, ir, icT);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Reconstruction: Wl, Wr at the interface between cell c and its +1
-// neighbour along DIR (update.cpp:247 / GPUupdate.cu:917-977).
+// neighbour along DIR, one interface per work item, the stencil read
+// straight from the state (used for the z sweep, where the lanes of a warp
+// are consecutive along the sweep and L1 serves the overlapping stencils).
 // ---------------------------------------------------------------------------
 template <int DIR, int PREC, int MINB>
 __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
@@ -121,66 +176,99 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
 #pragma unroll
             for (int q = 0; q < 5; ++q) s[a][q] = __ldg(f.W[q] + idx[a]);
         const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
-        double wl[5], wr[5];
-        if (PREC == 0) {
+        double T[6];
+        if (!direct) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                weno_pair<double>(s[0][q], s[1][q], s[2][q], s[3][q], s[4][q], s[5][q], kWenoEps, wl[q], wr[q]);
-            if (direct) {
-                weno_pair<double>(s[0][4], s[1][4], s[2][4], s[3][4], s[4][4], s[5][4], kWenoEps, wl[4], wr[4]);
-            } else {
-                double T[6];
-#pragma unroll
-                for (int a = 0; a < 6; ++a) T[a] = temperature(s[a], f.cT);
-                double tl, tr;
-                weno_pair<double>(T[0], T[1], T[2], T[3], T[4], T[5], kWenoEps, tl, tr);
-                // E from the reconstructed temperature (update.cpp:618-619)
-                const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
-                wl[4] = energy(wl, tl, il, f.icT);
-                wr[4] = energy(wr, tr, ir, f.icT);
-            }
-        } else {
-            // mixed: WENO in FP32 on differences from the left cell, added back
-            // in FP64; components (0, 1) and (2, 3) as the two lanes of paired
-            // FP32 instructions, the fifth (energy or temperature) alone
-            const float epsf = float(kWenoEps);
-#pragma unroll
-            for (int q = 0; q < 4; q += 2) {
-                const double c0 = s[2][q], c1 = s[2][q + 1];
-                f2 v[6];
-#pragma unroll
-                for (int a = 0; a < 6; ++a) v[a] = f2(float(s[a][q] - c0), float(s[a][q + 1] - c1));
-                f2 dl, dr;
-                weno_pair<f2>(v[0], v[1], f2(0.0f), v[3], v[4], v[5], f2(epsf), dl, dr);
-                wl[q] = c0 + double(dl.v.x);
-                wr[q] = c0 + double(dr.v.x);
-                wl[q + 1] = c1 + double(dl.v.y);
-                wr[q + 1] = c1 + double(dr.v.y);
-            }
-            if (direct) {
-                const double c0 = s[2][4];
-                float dl, dr;
-                weno_pair<float>(float(s[0][4] - c0), float(s[1][4] - c0), 0.0f, float(s[3][4] - c0),
-                                 float(s[4][4] - c0), float(s[5][4] - c0), epsf, dl, dr);
-                wl[4] = c0 + double(dl);
-                wr[4] = c0 + double(dr);
-            } else {
-                double T[6];
-#pragma unroll
-                for (int a = 0; a < 6; ++a) T[a] = temperature(s[a], f.cT);
-                float dl, dr;
-                weno_pair<float>(float(T[0] - T[2]), float(T[1] - T[2]), 0.0f, float(T[3] - T[2]),
-                                 float(T[4] - T[2]), float(T[5] - T[2]), epsf, dl, dr);
-                const double tl = T[2] + double(dl), tr = T[2] + double(dr);
-                const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
-                wl[4] = energy(wl, tl, il, f.icT);
-                wr[4] = energy(wr, tr, ir, f.icT);
-            }
+            for (int a = 0; a < 6; ++a) T[a] = temperature(s[a], f.cT);
         }
+        double wl[5], wr[5];
+        recon_point<PREC>(s, T, direct, f.icT, wl, wr);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             f.rec[q][x.c] = wl[q];
             f.rec[5 + q][x.c] = wr[q];
+        }
+    }
+}
+
+// Field of window item `it` (the last field whose window range starts at or before it).
+__device__ __forceinline__ int field_of_win(const FieldDev *f, int n, long long it)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (f[mid].wbase <= it) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Reconstruction for the x (DIR 0) and y (DIR 1) sweeps with a sliding
+// window: a work item is a run of win_run(PREC) consecutive interfaces along
+// the sweep at one (transverse line, k); the lanes of a warp take consecutive
+// k, so every load is coalesced.  The six stencil cells and their
+// temperatures stay in registers and move by one cell per interface: one new
+// cell (five loads) and one temperature per interface instead of thirty loads
+// and six temperatures.  Item order: k fastest, then run, then the transverse
+// line.  The loop is kept rolled (FP64) or unrolled twice (mixed): a fully
+// unrolled run holds several interfaces' loads and WENO temporaries at once
+// and needs more than 255 registers in FP64.
+// ---------------------------------------------------------------------------
+template <int DIR, int PREC, int MINB>
+__global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
+{
+    static_assert(DIR == 0 || DIR == 1, "windowed reconstruction is for the x and y sweeps");
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.wtotal; it += stride) {
+        const FieldDev &f = b.fields[field_of_win(b.fields, b.nfields, it)];
+        const long long loc = it - f.wbase;
+        if (loc >= f.nwin) continue; // alignment padding after the field
+        const int nc = f.nc;
+        const unsigned u = unsigned(loc);
+        const unsigned rest = div_nc(u, f);
+        const int k = int(u - rest * unsigned(nc));
+        const int line = int(rest / unsigned(f.nrun));
+        constexpr int RUN = win_run(PREC);
+        const int s0 = int(rest - unsigned(line) * unsigned(f.nrun)) * RUN;
+        // cell (line, sweep position p, k): x sweep (j, i, k), y sweep (j = p, i = line)
+        const unsigned step = DIR == 0 ? unsigned(nc) : unsigned(nc) * unsigned(nc);
+        const unsigned lbase = DIR == 0 ? unsigned(line) * unsigned(nc) * unsigned(nc) + unsigned(k)
+                                        : unsigned(line) * unsigned(nc) + unsigned(k);
+        auto cell = [&](int p) -> unsigned { return lbase + unsigned(wrap(p, nc)) * step; };
+        const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
+        double s[6][5], T[6];
+#pragma unroll
+        for (int a = 0; a < 5; ++a) {
+            const unsigned c = cell(s0 - 2 + a);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s[a + 1][q] = __ldg(f.W[q] + c);
+            T[a + 1] = direct ? 0.0 : temperature(s[a + 1], f.cT);
+        }
+        constexpr int UNROLL = PREC == 0 ? 1 : 2;
+#pragma unroll UNROLL
+        for (int r = 0; r < RUN; ++r) {
+            const int p = s0 + r;
+            if (p >= nc) break;
+            // slide: cells p-2 .. p+2 move down one slot, cell p+3 enters slot 5
+#pragma unroll
+            for (int a = 0; a < 5; ++a) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) s[a][q] = s[a + 1][q];
+                T[a] = T[a + 1];
+            }
+            const unsigned cn = cell(p + 3);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s[5][q] = __ldg(f.W[q] + cn);
+            T[5] = direct ? 0.0 : temperature(s[5], f.cT);
+            double wl[5], wr[5];
+            recon_point<PREC>(s, T, direct, f.icT, wl, wr);
+            const unsigned c = cell(p);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                f.rec[q][c] = wl[q];
+                f.rec[5 + q][c] = wr[q];
+            }
         }
     }
 }
@@ -733,19 +821,27 @@ cudaError_t occ(KernelT k, int block, int *n)
 }
 
 // Register-cap variants (min resident blocks per SM: reconstruction blocks of
-// 128 threads at 3 / 4 / 6 -> 168 / 128 / 80 registers, flux blocks of 64 threads at
+// 128 threads at 2 / 3 / 4 -> 255 / 168 / 128 registers, flux blocks of 64 threads at
 // 4 / 6 / 8 -> 255 / 168 / 128 registers); the tuner picks one per
 // kernel, precision and sweep.  Every variant gives bit-identical results.
-constexpr int kReconMinb[kReconVariants] = {3, 4, 6};
+constexpr int kReconMinb[kReconVariants] = {2, 3, 4};
 constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
 
 template <int DIR, int PREC>
 cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
 {
-    switch (cfg.variant) {
-    case 1: k_recon<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-    case 2: k_recon<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-    default: k_recon<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    if constexpr (DIR < 2) {
+        switch (cfg.variant) {
+        case 1: k_recon_win<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon_win<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        default: k_recon_win<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        }
+    } else {
+        switch (cfg.variant) {
+        case 1: k_recon<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        default: k_recon<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        }
     }
     return cudaGetLastError();
 }
@@ -764,7 +860,13 @@ cudaError_t flux_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
 template <int DIR, int PREC>
 cudaError_t occ_kind(int kind, int variant, int block, int *n)
 {
-    if (kind == K_RECON) {
+    if constexpr (DIR < 2) {
+        if (kind == K_RECON) {
+            if (variant == 1) return occ(k_recon_win<DIR, PREC, kReconMinb[1]>, block, n);
+            if (variant == 2) return occ(k_recon_win<DIR, PREC, kReconMinb[2]>, block, n);
+            return occ(k_recon_win<DIR, PREC, kReconMinb[0]>, block, n);
+        }
+    } else if (kind == K_RECON) {
         if (variant == 1) return occ(k_recon<DIR, PREC, kReconMinb[1]>, block, n);
         if (variant == 2) return occ(k_recon<DIR, PREC, kReconMinb[2]>, block, n);
         return occ(k_recon<DIR, PREC, kReconMinb[0]>, block, n);

@@ -22,6 +22,9 @@ struct FieldDev {
     const double *spl_inv;  // reciprocal pivots, nt entries
     long long base;   // first work item of this field in the batch (a multiple of kItemAlign)
     long long ncell;  // nc^3 (< 2^31)
+    long long wbase;  // first window item of this field (x / y reconstruction; a multiple of kItemAlign)
+    long long nwin;   // window items: nc^2 * nrun
+    int nrun;         // runs of win_run(prec) interfaces per line: ceil(nc / win_run(prec))
     int nc;
     unsigned nc_magic; // x / nc == (umulhi(x, nc_magic) + x) >> nc_shift for 32-bit x
     int nc_shift;
@@ -39,10 +42,15 @@ struct FieldDev {
 // kItemAlign consecutive items never spans two fields.
 constexpr int kItemAlign = 256;
 
+// Interfaces per work item of the windowed x / y reconstruction (prec 0 FP64,
+// 1 mixed; the lengths measured fastest on B200 at 256^3).
+__host__ __device__ constexpr int win_run(int prec) { return prec == 0 ? 64 : 32; }
+
 struct Batch {
     FieldDev *fields; // device array
     int nfields;
     long long total;  // end of the last field's item range
+    long long wtotal; // end of the last field's window item range
     int *err;         // device error word (bit 0: non-finite / non-positive state after update)
 };
 

@@ -359,6 +359,32 @@ def test_call_order_is_enforced(gks):
             s.upload(np.zeros((5, 10, 10, 10)))
 
 
+def test_grid_size_limits_are_enforced(gks, oracle):
+    """The stencil wraps the periodic box at most once (nc >= 4) and cell indices
+    are 32-bit (nc <= 1024): sizes outside are refused with GKS_EINVAL."""
+    case = gks_ic.make_dhit(8, seed=0)
+    for nc in (3, 1025):
+        p = gks.phys_from_case(case)
+        p.nc = nc
+        with pytest.raises(gks.GksError) as ei:
+            gks.Solver(p)
+        assert ei.value.code == -1
+    # the smallest box: every stencil wraps the periodic box, checked against the oracle
+    small = gks_ic.make_dhit(4, k0=2.0, Mt=0.2, seed=1)
+    W = gks_ic.to_conservative_padded(small)
+    with gks.Solver(gks.phys_from_case(small)) as s:
+        s.upload(W)
+        dt = s.timestep(0.5)
+        s.step(2)
+        s.sync()
+        got = s.download()
+    prm = oracle.params(4, small.gam, small.mu0, small.p0, 1.0, small.Mt, small.t0)
+    ref = W.copy()
+    oracle.step(ref, prm, dt, 2)
+    err = np.abs(got - ref).reshape(5, -1).max(1) / np.abs(ref).reshape(5, -1).max(1)
+    assert np.all(err < 1e-12), err
+
+
 def test_mixed_accuracy_to_two_eddy_times(gks):
     """Mixed vs FP64 at t/t0 = 2 (64^3, Mt 0.5, Re_lambda 100): KE and dissipation
     within 1e-5 relative, the precision target of the mixed path."""
