@@ -293,6 +293,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.gam = p.gam;
         d.gm1 = p.gam - 1;
         d.R = p.gas_r;
+        d.iR = 1.0 / p.gas_r;
         d.cT = (p.gam - 1) / p.gas_r;
         d.icT = p.gas_r / (p.gam - 1.0);
         d.T0 = p.T0;

@@ -159,6 +159,7 @@ __device__ __forceinline__ Prim prim(const double W[5], double gm1)
 struct FluxConst {
     double gm1;   // gamma - 1
     double dt, dx;
+    double ks[3]; // slope scales: 2/dx (normal), +-1/(2 dx) (transverse)
     double kA;    // pr_factor * 4 / (K + 3)
     int K;
 };

@@ -38,6 +38,8 @@
 
 namespace gks {
 
+constexpr double kHalfRsqrtPi = 0.28209479177387814; // 1 / (2 sqrt(pi))
+
 // Constants of one Maxwellian in its transverse co-moving frame.  The
 // negated copies let every use be a plain fused multiply-add, also for the
 // paired type f2, whose instructions take no operand negation.
@@ -200,9 +202,10 @@ __device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, 
     src.state(NEG, W);
     const Prim g = prim(W, c.gm1);
     {
-        const double sl = sqrt(g.lam);
+        // one reciprocal square root: sqrt(lambda) = lambda / sqrt(lambda)
+        const double rl = rsqrt(g.lam), sl = g.lam * rl;
         const double h0 = 0.5 * erfc(NEG ? sl * g.U0 : -sl * g.U0);
-        const double ex = 0.5 * exp(-g.lam * g.U0 * g.U0) * rsqrt(kPi * g.lam);
+        const double ex = exp(-g.lam * g.U0 * g.U0) * (kHalfRsqrtPi * rl);
         half_table<7>(g.U0, g.s, h0, NEG ? -ex : ex, Xh);
     }
     full_table<6, double>(g.U0, g.s, Xf);
@@ -220,15 +223,16 @@ __device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, 
 
 // Slope part of the side pass, on the arithmetic type T of the flux assembly:
 // double (one Maxwellian), or f2 (the left and right Maxwellians as the two
-// lanes of paired FP32 instructions).  `io` supplies the slopes,
-//   io.slope(d, b)        the slope vector along d = normal, 1st, 2nd transverse
+// lanes of paired FP32 instructions).  `io` supplies the state differences,
+//   io.slope(d, b)        along d = normal, 1st, 2nd transverse, which
+// sc[d] = ks[d] / rho turns into the right-hand sides b = DW / rho,
 // and takes the lab-frame results,
 //   io.emit(slot, den, M) adds den * M to S sum slot `slot` (lanes summed):
 // the transverse right-hand sides by_, bz_ of the equilibrium slopes (slots
 // 0-4, 5-9), B_ (10-14) and the p4 / p5 flux terms (15-19).
 template <typename T, typename IO>
-__device__ __forceinline__ void side_slopes(const IO &io, const CoFrame<T> &f, const T *Xh, const T *Xf, T rinv,
-                                            T den, T w45, T g5, T p4, T p5)
+__device__ __forceinline__ void side_slopes(const IO &io, const CoFrame<T> &f, const T *Xh, const T *Xf,
+                                            const T sc[3], T den, T w45, T g5, T p4, T p5)
 {
     // slope coefficients (phase I, GKMflux.cpp:102-117) and the moment sums they
     // feed, in the primed frame: Bm = -B -> A (phase II, GKMflux.cpp:128-144),
@@ -241,7 +245,7 @@ __device__ __forceinline__ void side_slopes(const IO &io, const CoFrame<T> &f, c
         // normal slope
         io.slope(0, b);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] *= rinv;
+        for (int q = 0; q < 5; ++q) b[q] *= sc[0];
         to_prime<T>(b, f);
         solve<T>(b, f, a);
         mom_n<1, T>(Bm, Xf, f, a);
@@ -250,7 +254,7 @@ __device__ __forceinline__ void side_slopes(const IO &io, const CoFrame<T> &f, c
         // first transverse slope (weight v = c1 + U1)
         io.slope(1, b);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] *= rinv;
+        for (int q = 0; q < 5; ++q) b[q] *= sc[1];
         to_prime<T>(b, f);
         solve<T>(b, f, a);
         acc_mom_t<0, 2, T>(Bm, Xf, f, a);
@@ -265,7 +269,7 @@ __device__ __forceinline__ void side_slopes(const IO &io, const CoFrame<T> &f, c
         // second transverse slope (weight w = c2 + U2)
         io.slope(2, b);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] *= rinv;
+        for (int q = 0; q < 5; ++q) b[q] *= sc[2];
         to_prime<T>(b, f);
         solve<T>(b, f, a);
         acc_mom_t<0, 3, T>(Bm, Xf, f, a);
@@ -345,13 +349,15 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
         double Xh[7], Xf[6];
         const Prim g = side_tables<0>(src, c, tw.p3, Xh, Xf);
         const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.K, c.kA);
-        side_slopes<double>(SideIO64<0, Src>{src}, f, Xh, Xf, g.rinv, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
+        const double sc[3] = {c.ks[0] * g.rinv, c.ks[1] * g.rinv, c.ks[2] * g.rinv};
+        side_slopes<double>(SideIO64<0, Src>{src}, f, Xh, Xf, sc, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
     }
     {
         double Xh[7], Xf[6];
         const Prim g = side_tables<1>(src, c, tw.p3, Xh, Xf);
         const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.K, c.kA);
-        side_slopes<double>(SideIO64<1, Src>{src}, f, Xh, Xf, g.rinv, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
+        const double sc[3] = {c.ks[0] * g.rinv, c.ks[1] * g.rinv, c.ks[2] * g.rinv};
+        side_slopes<double>(SideIO64<1, Src>{src}, f, Xh, Xf, sc, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
     }
     asm volatile("" ::: "memory");
 }
@@ -385,7 +391,8 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
         s.v.y = float(g.s); lam.v.y = float(g.lam); rinv.v.y = float(g.rinv); den.v.y = float(g.den);
     }
     const CoFrame<f2> f = co_frame<f2>(U0, U1, U2, s, lam, c.K, f2(float(c.kA)));
-    side_slopes<f2>(SideIO2<Src>{src}, f, Xh, Xf, rinv, den, f2(float(tw.w45)), f2(float(-tw.g5)),
+    const f2 sc[3] = {f2(float(c.ks[0])) * rinv, f2(float(c.ks[1])) * rinv, f2(float(c.ks[2])) * rinv};
+    side_slopes<f2>(SideIO2<Src>{src}, f, Xh, Xf, sc, den, f2(float(tw.w45)), f2(float(-tw.g5)),
                     f2(float(tw.p4)), f2(float(-tw.p5)));
     asm volatile("" ::: "memory");
 }
@@ -453,10 +460,10 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
     {
         // 0.5 erfc(-+x) from one evaluation at |x|: the far tail is computed
         // directly, the other value as 1 - tail (no cancellation)
-        const double sl = sqrt(e.lam);
+        const double rl = rsqrt(e.lam), sl = e.lam * rl;
         const double x = sl * e.U0;
         const double tail = 0.5 * erfc(fabs(x));
-        const double g = 0.5 * exp(-e.lam * e.U0 * e.U0) * rsqrt(kPi * e.lam);
+        const double g = exp(-e.lam * e.U0 * e.U0) * (kHalfRsqrtPi * rl);
         half_table<7>(e.U0, e.s, x >= 0.0 ? 1.0 - tail : tail, g, Xp);
         half_table<7>(e.U0, e.s, x >= 0.0 ? tail : 1.0 - tail, -g, Xn);
     }
@@ -488,7 +495,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
     {
         double WL[5], WR[5];
         src.cells(WL, WR);
-        const S k2 = S(2.0 * e.rinv / c.dx);
+        const S k2 = S(c.ks[0] * e.rinv); // 2 / (rho_e dx)
         S b[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) b[q] = S(We[q] - WL[q]) * k2;

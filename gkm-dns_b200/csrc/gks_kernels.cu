@@ -74,7 +74,7 @@ __device__ __forceinline__ double viscosity(const FieldDev &f, double T)
     const double x = T * f.iT0;
     if (f.visc_law == GKS_VISC_POWER) return f.mu0 * pow(x, f.visc_exp);
     // mu0 (T/T0)^1.5 (T0 + 110.4)/(T + 110.4), update.cpp:263
-    return f.mu0 * (x * sqrt(x)) * (f.T0 + 110.4) / (T + 110.4);
+    return f.mu0 * (x * sqrt(x)) * (f.T0 + 110.4) * __drcp_rn(T + 110.4);
 }
 
 __device__ __forceinline__ double temperature(const double W[5], double cT)
@@ -325,12 +325,12 @@ struct SweepSrc {
     }
 
     // DWxl = 2(Wl - WL)/dx, DWxr = 2(WR - Wr)/dx; transverse central differences of
-    // the neighbouring lines' states (update.cpp:253-260, 327-334, 416-423)
+    // the neighbouring lines' states (update.cpp:253-260, 327-334, 416-423), here
+    // the differences, which the flux scales by FluxConst::ks
     __device__ __forceinline__ void load(const FieldDev &f, unsigned c, unsigned c1, unsigned cn, unsigned cs,
                                          unsigned cf, unsigned cb)
     {
-        // differences in double (they cancel), scaled in S
-        const S kn = S(2.0 * f.inv_dx), kt = S(0.5 * f.inv_dx), ky = DIR == 1 ? -kt : kt;
+        // differences in double (they cancel); the flux scales them (FluxConst::ks)
         const int t = threadIdx.x;
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -339,12 +339,12 @@ struct SweepSrc {
             const double wL = __ldg(f.W[o] + c), wR = __ldg(f.W[o] + c1);
             const double wr = __ldg(rr + c);
             Wl[q] = __ldg(rl + c);
-            DWl[0][q] = kn * S(Wl[q] - wL);
-            DWl[1][q] = ky * S(__ldg(rl + cn) - __ldg(rl + cs));
-            DWl[2][q] = kt * S(__ldg(rl + cf) - __ldg(rl + cb));
-            park_dw[q][t] = kn * S(wR - wr);
-            park_dw[5 + q][t] = ky * S(__ldg(rr + cn) - __ldg(rr + cs));
-            park_dw[10 + q][t] = kt * S(__ldg(rr + cf) - __ldg(rr + cb));
+            DWl[0][q] = S(Wl[q] - wL);
+            DWl[1][q] = S(__ldg(rl + cn) - __ldg(rl + cs));
+            DWl[2][q] = S(__ldg(rl + cf) - __ldg(rl + cb));
+            park_dw[q][t] = S(wR - wr);
+            park_dw[5 + q][t] = S(__ldg(rr + cn) - __ldg(rr + cs));
+            park_dw[10 + q][t] = S(__ldg(rr + cf) - __ldg(rr + cb));
             park_w[q][t] = wL;
             park_w[5 + q][t] = wR;
             park_w[10 + q][t] = wr;
@@ -424,13 +424,16 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
             for (int q = 0; q < 5; ++q) w[SweepSrc<DIR, S>::perm(q)] = WL[q];
             const double ri = __drcp_rn(w[0]);
             const double P = f.gm1 * fma(-0.5 * fma(w[1], w[1], fma(w[2], w[2], w[3] * w[3])), ri, w[4]);
-            const double T = P * ri * (1.0 / f.R);
+            const double T = P * ri * f.iR;
             tau0 = viscosity(f, T) * __drcp_rn(P);
         }
         FluxConst fc;
         fc.gm1 = f.gm1;
         fc.dt = f.dt;
         fc.dx = f.dx;
+        fc.ks[0] = 2.0 * f.inv_dx;
+        fc.ks[1] = (DIR == 1 ? -0.5 : 0.5) * f.inv_dx; // y sweep: DWy = -(N - S)/(2 dx)
+        fc.ks[2] = 0.5 * f.inv_dx;
         fc.kA = f.kA;
         fc.K = f.K;
         double F[5];

@@ -32,7 +32,7 @@ struct FieldDev {
     int visc_law;     // 0 Sutherland, 1 power law
     int flags;        // GKS_FIX_ZSWEEP | GKS_DIRECT_ENERGY
     double dx, inv_dx, dt;
-    double gam, gm1, R, cT, icT; // cT = (gam-1)/R, icT = R/(gam-1)
+    double gam, gm1, R, iR, cT, icT; // iR = 1/R, cT = (gam-1)/R, icT = R/(gam-1)
     double T0, iT0, mu0, visc_exp;
     double kA;        // pr_factor * 4/(K+3)
     double spl_s;     // 3/h of the spline grid
