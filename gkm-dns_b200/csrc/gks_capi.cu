@@ -245,6 +245,15 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     ctx->own_stream = true;
 
     ctx->fh.resize(nfields);
+    // run length of the windowed reconstruction: the longest that leaves the
+    // batch at least kWinItemsPerSm window items per SM
+    int run = gks::win_run(precision == GKS_MIXED ? 1 : 0);
+    for (; run > gks::kWinRunMin; run /= 2) {
+        long long items = 0;
+        for (int f = 0; f < nfields; ++f)
+            items += (long long)phys[f].nc * phys[f].nc * ((phys[f].nc + run - 1) / run);
+        if (items >= (long long)gks::kWinItemsPerSm * ctx->nsm) break;
+    }
     long long base = 0, wbase = 0;
     const double pi = std::atan(1.0) * 4.0; // param.h:14
     for (int f = 0; f < nfields; ++f) {
@@ -270,7 +279,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.base = base;
         d.ncell = n;
         base += (n + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
-        const int run = gks::win_run(precision == GKS_MIXED ? 1 : 0);
+        d.run = run;
         d.nrun = (p.nc + run - 1) / run;
         d.nwin = (long long)p.nc * p.nc * d.nrun;
         d.wbase = wbase;

@@ -205,8 +205,8 @@ __device__ __forceinline__ int field_of_win(const FieldDev *f, int n, long long 
 
 // ---------------------------------------------------------------------------
 // Reconstruction for the x (DIR 0) and y (DIR 1) sweeps with a sliding
-// window: a work item is a run of win_run(PREC) consecutive interfaces along
-// the sweep at one (transverse line, k); the lanes of a warp take consecutive
+// window: a work item is a run of f.run consecutive interfaces along the
+// sweep at one (transverse line, k); the lanes of a warp take consecutive
 // k, so every load is coalesced.  The six stencil cells and their
 // temperatures stay in registers and move by one cell per interface: one new
 // cell (five loads) and one temperature per interface instead of thirty loads
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
         const unsigned rest = div_nc(u, f);
         const int k = int(u - rest * unsigned(nc));
         const int line = int(rest / unsigned(f.nrun));
-        constexpr int RUN = win_run(PREC);
+        const int RUN = f.run;
         const int s0 = int(rest - unsigned(line) * unsigned(f.nrun)) * RUN;
         // cell (line, sweep position p, k): x sweep (j, i, k), y sweep (j = p, i = line)
         const unsigned step = DIR == 0 ? unsigned(nc) : unsigned(nc) * unsigned(nc);

@@ -24,7 +24,8 @@ struct FieldDev {
     long long ncell;  // nc^3 (< 2^31)
     long long wbase;  // first window item of this field (x / y reconstruction; a multiple of kItemAlign)
     long long nwin;   // window items: nc^2 * nrun
-    int nrun;         // runs of win_run(prec) interfaces per line: ceil(nc / win_run(prec))
+    int run;          // interfaces per window item (the same for every field of a batch)
+    int nrun;         // runs per line: ceil(nc / run)
     int nc;
     unsigned nc_magic; // x / nc == (umulhi(x, nc_magic) + x) >> nc_shift for 32-bit x
     int nc_shift;
@@ -42,9 +43,13 @@ struct FieldDev {
 // kItemAlign consecutive items never spans two fields.
 constexpr int kItemAlign = 256;
 
-// Interfaces per work item of the windowed x / y reconstruction (prec 0 FP64,
-// 1 mixed; the lengths measured fastest on B200 at 256^3).
+// Longest run of interfaces per work item of the windowed x / y
+// reconstruction (prec 0 FP64, 1 mixed; the lengths measured fastest on B200
+// at 256^3).  A batch halves it, down to kWinRunMin, while it has fewer than
+// kWinItemsPerSm items per SM, so that small fields still fill the GPU.
 __host__ __device__ constexpr int win_run(int prec) { return prec == 0 ? 64 : 32; }
+constexpr int kWinRunMin = 8;
+constexpr int kWinItemsPerSm = 768;
 
 struct Batch {
     FieldDev *fields; // device array
