@@ -149,7 +149,7 @@ gks::LaunchCfg persistent(gks_ctx *ctx, int kind, int dir, int variant, int mult
     if (gks::max_resident_blocks(kind, dir, ctx->precision, variant, c.block, &per_sm) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     long long g = (long long)ctx->nsm * per_sm * mult;
-    const long long items = (kind == gks::K_RECON && dir < 2) ? ctx->batch.wtotal : ctx->batch.total;
+    const long long items = (kind == gks::K_RECON && dir < 2 && variant < 3) ? ctx->batch.wtotal : ctx->batch.total;
     const long long need = (items + c.block - 1) / c.block;
     if (g > need) g = need;
     if (g < 1) g = 1;

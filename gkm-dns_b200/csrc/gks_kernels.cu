@@ -559,10 +559,10 @@ __global__ void k_velocity(FieldDev f, double *scr)
     const long long n = f.ncell;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
-        const double d = f.W[0][c];
-        scr[c] = f.W[1][c] / d;
-        scr[n + c] = f.W[2][c] / d;
-        scr[2 * n + c] = f.W[3][c] / d;
+        const double ri = __drcp_rn(f.W[0][c]);
+        scr[c] = f.W[1][c] * ri;
+        scr[n + c] = f.W[2][c] * ri;
+        scr[2 * n + c] = f.W[3][c] * ri;
     }
 }
 
@@ -592,17 +592,21 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
     if (line0 >= lines) return; // uniform per warp
     const int nl = int(min((long long)kSplLines, lines - line0));
     const long long st = axis == 0 ? (long long)nc * nc : (axis == 1 ? (long long)nc : 1LL);
-    auto base_of = [&](int l) -> long long {
-        const long long L = line0 + l;
-        const long long a = L / nc, b = L % nc;
-        return axis == 0 ? a * nc + b : (axis == 1 ? a * nc * nc + b : (a * nc + b) * nc); // (i,k), (j,k), (j,i)
-    };
     const bool mine = lane < nl;
-    const long long mybase = base_of(mine ? lane : 0);
+    // first cell of this lane's line: (i,k), (j,k) or (j,i) lines for axis 0, 1, 2;
+    // a lane reads another line's base with a shuffle
+    long long mybase;
+    {
+        const long long L = line0 + (mine ? lane : 0);
+        const long long a = L / nc, b = L - a * nc;
+        mybase = axis == 0 ? a * nc + b : (axis == 1 ? a * nc * nc + b : (a * nc + b) * nc);
+    }
     const double s = f.spl_s;
     const double *cp = f.spl_cp, *inv = f.spl_inv;
     // node p of a line sits at cell wrap(p - 3) along the axis
     auto node_off = [&](int p) -> long long { return (long long)wrap(p - 3, nc) * st; };
+    // Every chunk's loads are issued before any of them is used (fully
+    // unrolled, predicated), so a chunk costs one memory latency, not one per node.
 
 #pragma unroll 1
     for (int comp = 0; comp < 3; ++comp) {
@@ -613,18 +617,18 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
 #pragma unroll 1
         for (int p0 = 0; p0 < nt; p0 += kSplChunk) {
             if (axis == 2) {
-                for (int l = 0; l < nl; ++l) {
-                    const long long b = base_of(l);
-                    for (int jj = lane; jj < kSplChunk + 2; jj += 32) {
-                        const int p = p0 - 1 + jj;
-                        if (p >= 0 && p < nt) tile[l][jj] = u[b + node_off(p)];
-                    }
+#pragma unroll
+                for (int l = 0; l < kSplLines; ++l) {
+                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                    const int p = p0 - 1 + lane;
+                    if (l < nl && p >= 0 && p < nt) tile[l][lane] = __ldg(u + b + node_off(p));
+                    if (lane < 2 && l < nl && p + 32 < nt) tile[l][lane + 32] = __ldg(u + b + node_off(p + 32));
                 }
             } else if (mine) {
-#pragma unroll 4
+#pragma unroll
                 for (int jj = 0; jj < kSplChunk + 2; ++jj) {
                     const int p = p0 - 1 + jj;
-                    if (p >= 0 && p < nt) tile[lane][jj] = u[mybase + node_off(p)];
+                    if (p >= 0 && p < nt) tile[lane][jj] = __ldg(u + mybase + node_off(p));
                 }
             }
             __syncwarp();
@@ -648,13 +652,14 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
             __syncwarp();
             // park forward values of nodes 3 .. nt-4 at cell p - 3
             if (axis == 2) {
-                for (int l = 0; l < nl; ++l) {
-                    const long long b = base_of(l);
-                    const int p = p0 + lane;
-                    if (p >= 3 && p <= nt - 4) g[b + (long long)(p - 3)] = tile[l][lane];
+                const int p = p0 + lane;
+#pragma unroll
+                for (int l = 0; l < kSplLines; ++l) {
+                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                    if (l < nl && p >= 3 && p <= nt - 4) g[b + (long long)(p - 3)] = tile[l][lane];
                 }
             } else if (mine) {
-#pragma unroll 4
+#pragma unroll
                 for (int c = 0; c < kSplChunk; ++c) {
                     const int p = p0 + c;
                     if (p >= 3 && p <= nt - 4) g[mybase + (long long)(p - 3) * st] = tile[lane][c];
@@ -670,11 +675,15 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
         for (int q0 = ((nc - 1) / kSplChunk) * kSplChunk; q0 >= 0; q0 -= kSplChunk) {
             const int cnt = min(kSplChunk, nc - q0);
             if (axis == 2) {
-                for (int l = 0; l < nl; ++l)
-                    if (lane < cnt) tile[l][lane] = g[base_of(l) + (long long)(q0 + lane)];
+#pragma unroll
+                for (int l = 0; l < kSplLines; ++l) {
+                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                    if (l < nl && lane < cnt) tile[l][lane] = g[b + (long long)(q0 + lane)];
+                }
             } else if (mine) {
-#pragma unroll 4
-                for (int c = 0; c < cnt; ++c) tile[lane][c] = g[mybase + (long long)(q0 + c) * st];
+#pragma unroll
+                for (int c = 0; c < kSplChunk; ++c)
+                    if (c < cnt) tile[lane][c] = g[mybase + (long long)(q0 + c) * st];
             }
             __syncwarp();
             if (mine) {
@@ -685,11 +694,15 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
             }
             __syncwarp();
             if (axis == 2) {
-                for (int l = 0; l < nl; ++l)
-                    if (lane < cnt) g[base_of(l) + (long long)(q0 + lane)] = tile[l][lane];
+#pragma unroll
+                for (int l = 0; l < kSplLines; ++l) {
+                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                    if (l < nl && lane < cnt) g[b + (long long)(q0 + lane)] = tile[l][lane];
+                }
             } else if (mine) {
-#pragma unroll 4
-                for (int c = 0; c < cnt; ++c) g[mybase + (long long)(q0 + c) * st] = tile[lane][c];
+#pragma unroll
+                for (int c = 0; c < kSplChunk; ++c)
+                    if (c < cnt) g[mybase + (long long)(q0 + c) * st] = tile[lane][c];
             }
             __syncwarp();
         }
@@ -723,16 +736,19 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *out)
     }
 }
 
-__device__ __forceinline__ void cell_prim(const FieldDev &f, long long c, double &den, double &u, double &v,
-                                          double &w, double &P, double &T)
+// Primitive state of a cell (c2p, update.cpp:882-891) with one reciprocal of
+// the density; ri = 1/rho.
+__device__ __forceinline__ void cell_prim(const FieldDev &f, long long c, double &den, double &ri, double &u,
+                                          double &v, double &w, double &P, double &T)
 {
     den = f.W[0][c];
-    u = f.W[1][c] / den;
-    v = f.W[2][c] / den;
-    w = f.W[3][c] / den;
-    const double vsq = u * u + v * v + w * w;
-    P = (den * f.gm1) * (f.W[4][c] / den - 0.5 * vsq);
-    T = P / (f.R * den);
+    ri = __drcp_rn(den);
+    u = f.W[1][c] * ri;
+    v = f.W[2][c] * ri;
+    w = f.W[3][c] * ri;
+    const double vsq = fma(u, u, fma(v, v, w * w));
+    P = (den * f.gm1) * fma(-0.5, vsq, f.W[4][c] * ri);
+    T = P * ri * f.iR;
 }
 
 __global__ void k_sums1(FieldDev f, const double *scr, double *partial)
@@ -743,8 +759,8 @@ __global__ void k_sums1(FieldDev f, const double *scr, double *partial)
     for (int i = 0; i < NSUM1; ++i) acc[i] = 0.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
-        double den, u, v, w, P, T;
-        cell_prim(f, c, den, u, v, w, P, T);
+        double den, ri, u, v, w, P, T;
+        cell_prim(f, c, den, ri, u, v, w, P, T);
         const double *g = scr + 3 * n;
         const double dudy = g[c], dudx = g[n + c], dudz = g[2 * n + c];
         const double dvdy = g[3 * n + c], dvdx = g[4 * n + c], dvdz = g[5 * n + c];
@@ -761,9 +777,9 @@ __global__ void k_sums1(FieldDev f, const double *scr, double *partial)
         acc[9] += c2; acc[10] += c2 * dwdz; acc[11] += c2 * c2;
         acc[12] += P;
         acc[13] += T;
-        acc[14] += 1.0 / den;
+        acc[14] += ri;
         acc[15] += u * u + v * v + w * w;
-        acc[16] += sqrt(f.gam * P / den);
+        acc[16] += sqrt(f.gam * P * ri);
         acc[17] += den;
     }
     block_sums<NSUM1>(acc, partial + (long long)blockIdx.x * NSUM1);
@@ -776,11 +792,11 @@ __global__ void k_sums2(FieldDev f, const double *means, double *partial)
     double acc[NSUM2] = {0.0, 0.0, 0.0};
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
-        double den, u, v, w, P, T;
-        cell_prim(f, c, den, u, v, w, P, T);
+        double den, ri, u, v, w, P, T;
+        cell_prim(f, c, den, ri, u, v, w, P, T);
         acc[0] += (Pm - P) * (Pm - P);
         acc[1] += (Tm - T) * (Tm - T);
-        acc[2] += (Vm - 1.0 / den) * (Vm - 1.0 / den);
+        acc[2] += (Vm - ri) * (Vm - ri);
     }
     block_sums<NSUM2>(acc, partial + (long long)blockIdx.x * NSUM2);
 }
@@ -824,23 +840,27 @@ cudaError_t occ(KernelT k, int block, int *n)
 }
 
 // Register-cap variants (min resident blocks per SM: reconstruction blocks of
-// 128 threads at 2 / 3 / 4 -> 255 / 168 / 128 registers, flux blocks of 64 threads at
+// 128 threads at 2 / 3 / 4 -> 255 / 168 / 128 registers, each in the windowed
+// and the one-interface form, flux blocks of 64 threads at
 // 4 / 6 / 8 -> 255 / 168 / 128 registers); the tuner picks one per
 // kernel, precision and sweep.  Every variant gives bit-identical results.
-constexpr int kReconMinb[kReconVariants] = {2, 3, 4};
+constexpr int kReconMinb[3] = {2, 3, 4};
 constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
 
+// Reconstruction variants: 0-2 the windowed kernel (x, y sweeps) at the three
+// register caps, 3-5 the one-interface-per-thread kernel at the same caps (the
+// z sweep always runs the latter).
 template <int DIR, int PREC>
 cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
 {
-    if constexpr (DIR < 2) {
+    if (DIR < 2 && cfg.variant < 3) {
         switch (cfg.variant) {
-        case 1: k_recon_win<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        case 2: k_recon_win<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        default: k_recon_win<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 1: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        default: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
         }
     } else {
-        switch (cfg.variant) {
+        switch (cfg.variant % 3) {
         case 1: k_recon<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
         case 2: k_recon<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
         default: k_recon<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
@@ -863,15 +883,15 @@ cudaError_t flux_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
 template <int DIR, int PREC>
 cudaError_t occ_kind(int kind, int variant, int block, int *n)
 {
-    if constexpr (DIR < 2) {
-        if (kind == K_RECON) {
-            if (variant == 1) return occ(k_recon_win<DIR, PREC, kReconMinb[1]>, block, n);
-            if (variant == 2) return occ(k_recon_win<DIR, PREC, kReconMinb[2]>, block, n);
-            return occ(k_recon_win<DIR, PREC, kReconMinb[0]>, block, n);
-        }
-    } else if (kind == K_RECON) {
-        if (variant == 1) return occ(k_recon<DIR, PREC, kReconMinb[1]>, block, n);
-        if (variant == 2) return occ(k_recon<DIR, PREC, kReconMinb[2]>, block, n);
+    if (kind == K_RECON && DIR < 2 && variant < 3) {
+        constexpr int D = DIR < 2 ? DIR : 0;
+        if (variant == 1) return occ(k_recon_win<D, PREC, kReconMinb[1]>, block, n);
+        if (variant == 2) return occ(k_recon_win<D, PREC, kReconMinb[2]>, block, n);
+        return occ(k_recon_win<D, PREC, kReconMinb[0]>, block, n);
+    }
+    if (kind == K_RECON) {
+        if (variant % 3 == 1) return occ(k_recon<DIR, PREC, kReconMinb[1]>, block, n);
+        if (variant % 3 == 2) return occ(k_recon<DIR, PREC, kReconMinb[2]>, block, n);
         return occ(k_recon<DIR, PREC, kReconMinb[0]>, block, n);
     }
     if (variant == 1) return occ(k_flux<DIR, PREC, kFluxMinb[1]>, block, n);

@@ -68,7 +68,7 @@ struct LaunchCfg {
 };
 
 enum KernelKind { K_RECON = 0, K_FLUX = 1, K_UPDATE = 2, K_KINDS = 3 };
-constexpr int kReconVariants = 3;
+constexpr int kReconVariants = 6;
 constexpr int kFluxVariants = 3;
 
 // Threads per block of each kernel kind.

@@ -305,7 +305,7 @@ def test_every_kernel_variant_gives_identical_results(gks, prec):
             return s.download()
 
     base = run([])
-    for kind, nvar in (("recon", 3), ("flux", 3)):
+    for kind, nvar in (("recon", 6), ("flux", 3)):
         for v in range(nvar):
             for grid in (0, 1):
                 got = run([(kind, v, grid)])
