@@ -61,18 +61,27 @@ def dist_env():
 
 
 class Dist:
-    def __init__(self, ws, local):
+    """Ranks of a replicas-only run: one process per GPU over NCCL (the
+    bench), or over gloo on CPU (tests).  Every rank takes the same
+    collective steps: barriers around the timed regions and a max over ranks
+    of each timing."""
+
+    def __init__(self, ws, local, backend: str = "nccl"):
         self.ws = ws
         self.pg = None
+        self.device = "cpu" if backend == "gloo" else "cuda"
         if ws > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", local))
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                        device_id=torch.device("cuda", local))
+            else:
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
@@ -84,7 +93,7 @@ class Dist:
             return x
         import torch
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -92,6 +101,12 @@ class Dist:
         if self.pg:
             self.pg.barrier()
             self.pg.destroy_process_group()
+
+
+def whole_job_rate(ws: int, cells_per_rank: int, max_ms: float) -> float:
+    """Cell-updates/s of the whole job: every rank advances its own replica of
+    `cells_per_rank` cells per step; the step time is the slowest rank's."""
+    return ws * cells_per_rank / (max_ms * 1e-3)
 
 
 class ClockSampler:
@@ -410,7 +425,7 @@ def run_ours(args):
         ens["fp64"]["ms_per_step"] = dist.max(ens["fp64"]["ms_per_step"])
         ens["mixed"]["ms_per_step"] = dist.max(ens["mixed"]["ms_per_step"])
         for k in ("fp64", "mixed"):
-            ens[k]["value"] = ws * ens["cells_per_step"] / (ens[k]["ms_per_step"] * 1e-3)
+            ens[k]["value"] = whole_job_rate(ws, ens["cells_per_step"], ens[k]["ms_per_step"])
 
     # e2e through the reference-facing call: upload from pinned host, step, download
     nt = nc + 6
@@ -438,8 +453,8 @@ def run_ours(args):
     bytes_io = 5 * nt ** 3 * 8
 
     cells = nc ** 3
-    value = ws * cells / (results["fp64"]["ms"] * 1e-3)
-    mixed_value = ws * cells / (results["mixed"]["ms"] * 1e-3)
+    value = whole_job_rate(ws, cells, results["fp64"]["ms"])
+    mixed_value = whole_job_rate(ws, cells, results["mixed"]["ms"])
     flux_ms = statistics.mean(stages["fp64"][k] for k in ("flux_x", "flux_y", "flux_z"))
     recon_ms = statistics.mean(stages["fp64"][k] for k in ("recon_x", "recon_y", "recon_z"))
     achieved = OPS_FLUX * cells / (flux_ms * 1e-3) / 1e12
@@ -493,7 +508,7 @@ def run_ours(args):
             "ensemble": ens,
             "launch": {"fp64": results["fp64"]["launch"], "mixed": results["mixed"]["launch"],
                        "tuned": not args.no_tune},
-            "e2e": {"value": ws * cells / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+            "e2e": {"value": whole_job_rate(ws, cells, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms,
                     "call": "gks_upload + gks_step(1) + gks_download per step, pinned host buffers"},
             "clocks": results["fp64"]["clocks"],
