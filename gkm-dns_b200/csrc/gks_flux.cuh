@@ -320,10 +320,12 @@ struct SideIO64 {
     }
 };
 
-// Slope inputs and results of the paired side pass (left lane .x, right .y).
+// Slope inputs and results of the paired side pass (left lane .x, right .y);
+// the lane-summed results stay in the caller's registers (out[20]).
 template <typename Src>
 struct SideIO2 {
     const Src &src;
+    float *out;
     __device__ __forceinline__ void slope(int d, f2 b[5]) const
     {
         float l[5], r[5];
@@ -334,7 +336,7 @@ struct SideIO2 {
     }
     __device__ __forceinline__ void emit(int slot, f2 a, f2 m) const
     {
-        src.put_raw_s(slot, __fmaf_rn(a.v.y, m.v.y, __fmul_rn(a.v.x, m.v.x)));
+        out[slot] = __fmaf_rn(a.v.y, m.v.y, __fmul_rn(a.v.x, m.v.x));
     }
 };
 
@@ -343,7 +345,7 @@ struct SideIO2 {
 // scheduler cannot start its long erfc / exp chains early and keep the side
 // passes' state live at the same time.
 template <typename Src>
-__device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, const SideWeights &tw, double)
+__device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, const SideWeights &tw, double, float *)
 {
     {
         double Xh[7], Xf[6];
@@ -366,7 +368,7 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
 // chains overlap), then their FP32 slope parts together as the lanes of
 // paired instructions.
 template <typename Src>
-__device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, const SideWeights &tw, float)
+__device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, const SideWeights &tw, float, float *sout)
 {
     f2 Xh[7], Xf[6];
     f2 U0, U1, U2, s, lam, rinv, den;
@@ -392,7 +394,7 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
     }
     const CoFrame<f2> f = co_frame<f2>(U0, U1, U2, s, lam, c.K, f2(float(c.kA)));
     const f2 sc[3] = {f2(float(c.ks[0])) * rinv, f2(float(c.ks[1])) * rinv, f2(float(c.ks[2])) * rinv};
-    side_slopes<f2>(SideIO2<Src>{src}, f, Xh, Xf, sc, den, f2(float(tw.w45)), f2(float(-tw.g5)),
+    side_slopes<f2>(SideIO2<Src>{src, sout}, f, Xh, Xf, sc, den, f2(float(tw.w45)), f2(float(-tw.g5)),
                     f2(float(tw.p4)), f2(float(-tw.p5)));
     asm volatile("" ::: "memory");
 }
@@ -412,6 +414,8 @@ __device__ __forceinline__ double pressure(const double W[5], double gm1)
 //   src.slope(side, d, DW)    its slopes along d = normal, 1st, 2nd transverse
 //   src.cells(WL, WR)         the cell averages either side of the interface
 //   src.put_d / put_s<FIRST>(slot, v), get_d / get_s(slot)   running sums
+// (the mixed path keeps its type-S sums in registers: the paired side pass
+// produces them all at once).
 // tau0 = mu/p at the left cell.  Output F[5], the flux integrated over [0, dt].
 template <typename S, typename Src>
 __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const FluxConst &c, double F[5])
@@ -442,7 +446,12 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         tw.p4 = fma(-tau, Pt, -Qt);
         tw.p5 = -tau * Pt;
     }
-    flux_sides(src, c, tw, S());
+    float sreg[20];
+    flux_sides(src, c, tw, S(), sreg);
+    auto gets = [&](int k) -> S {
+        if constexpr (sizeof(S) == 4) return sreg[k];
+        else return src.get_s(k);
+    };
     const double gm1 = -om * igm0, gm3 = -gm1;
     const double Pt = tau * om, Qt = tau * fma(-dt, ex, Pt);
     const double gm2 = fma(-dt, ex, fma(2.0, Pt, -dt)) * igm0;
@@ -477,7 +486,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         mom0_lab<0>(M, Xf, e, c4);
         const double w = gm1 * e.den;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Bd[q] = (fma(w, M[q], gm3 * We[q]) + double(src.get_s(10 + q))) * e.rinv;
+        for (int q = 0; q < 5; ++q) Bd[q] = (fma(w, M[q], gm3 * We[q]) + double(gets(10 + q))) * e.rinv;
         to_prime<double>(Bd, -e.U1, -e.U2, -0.5 * fma(e.U1, e.U1, e.U2 * e.U2));
     }
     const CoFrame<S> f = co_frame<S>(S(e.U0), S(e.U1), S(e.U2), S(e.s), S(e.lam), c.K, S(c.kA));
@@ -506,11 +515,11 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         to_prime<S>(b, f);
         solve<S>(b, f, axr);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] = src.get_s(q);
+        for (int q = 0; q < 5; ++q) b[q] = gets(q);
         to_prime<S>(b, f);
         solve<S>(b, f, ay);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) b[q] = src.get_s(5 + q);
+        for (int q = 0; q < 5; ++q) b[q] = gets(5 + q);
         to_prime<S>(b, f);
         solve<S>(b, f, az);
 #pragma unroll
@@ -552,7 +561,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         const double w0 = p0 * e.den;
 #pragma unroll
         for (int q = 0; q < 5; ++q)
-            F[q] = fma(w0, M0[q], src.get_d(5 + q)) + double(fmaT(dens, T1[q], src.get_s(15 + q)));
+            F[q] = fma(w0, M0[q], src.get_d(5 + q)) + double(fmaT(dens, T1[q], gets(15 + q)));
     }
 }
 

@@ -317,7 +317,7 @@ struct SweepSrc {
     S (*park_dw)[kFluxBlock];      // [15][block]: right-side slopes
     double (*park_w)[kFluxBlock];  // [15][block]: WL, WR, Wr
     double (*sum_d)[kFluxBlock];   // [10][block]: double sums of the side passes
-    S (*sum_s)[kFluxBlock];        // [20][block]: S sums of the side passes
+    S (*sum_s)[kFluxBlock];        // [20][block]: S sums of the side passes (FP64 path)
 
     __device__ static constexpr int perm(int q)
     {
@@ -388,7 +388,6 @@ struct SweepSrc {
         if constexpr (sizeof(S) == 8) x = FIRST ? __dmul_rn(a, b) : __fma_rn(a, b, x);
         else x = FIRST ? __fmul_rn(a, b) : __fmaf_rn(a, b, x);
     }
-    __device__ __forceinline__ void put_raw_s(int i, S v) const { sum_s[i][threadIdx.x] = v; }
     __device__ __forceinline__ double get_d(int i) const { return sum_d[i][threadIdx.x]; }
     __device__ __forceinline__ S get_s(int i) const { return sum_s[i][threadIdx.x]; }
 };
