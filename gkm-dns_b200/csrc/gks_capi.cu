@@ -149,7 +149,11 @@ gks::LaunchCfg persistent(gks_ctx *ctx, int kind, int dir, int variant, int mult
     if (gks::max_resident_blocks(kind, dir, ctx->precision, variant, c.block, &per_sm) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     long long g = (long long)ctx->nsm * per_sm * mult;
-    const long long items = (kind == gks::K_RECON && dir < 2 && variant < 3) ? ctx->batch.wtotal : ctx->batch.total;
+    // work items: window runs (x / y reconstruction variants 0-2), warp-sized
+    // z segments of 32 threads each (z reconstruction variants 0-2), else cells
+    const long long items = (kind == gks::K_RECON && variant < 3)
+                                ? (dir < 2 ? ctx->batch.wtotal : ctx->batch.ztotal * 32)
+                                : ctx->batch.total;
     const long long need = (items + c.block - 1) / c.block;
     if (g > need) g = need;
     if (g < 1) g = 1;
@@ -254,7 +258,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
             items += (long long)phys[f].nc * phys[f].nc * ((phys[f].nc + run - 1) / run);
         if (items >= (long long)gks::kWinItemsPerSm * ctx->nsm) break;
     }
-    long long base = 0, wbase = 0;
+    long long base = 0, wbase = 0, zbase = 0;
     const double pi = std::atan(1.0) * 4.0; // param.h:14
     for (int f = 0; f < nfields; ++f) {
         FieldHost &h = ctx->fh[f];
@@ -284,6 +288,9 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.nwin = (long long)p.nc * p.nc * d.nrun;
         d.wbase = wbase;
         wbase += (d.nwin + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
+        d.nzseg = (long long)p.nc * p.nc * ((p.nc + 31) / 32);
+        d.zbase = zbase;
+        zbase += d.nzseg;
         d.nc = p.nc;
         // magic number for x / nc (round-up method): l = ceil(log2 nc),
         // m = floor(2^32 (2^l - nc) / nc) + 1, x / nc = (umulhi(x, m) + x) >> l
@@ -327,6 +334,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     ctx->batch.nfields = nfields;
     ctx->batch.total = base;
     ctx->batch.wtotal = wbase;
+    ctx->batch.ztotal = zbase;
     ctx->batch.err = ctx->d_err;
     choose_launch(ctx);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(GKS_ECUDA);

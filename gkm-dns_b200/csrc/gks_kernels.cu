@@ -191,6 +191,80 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
     }
 }
 
+// Field of z-segment item `it` (the last field whose segment range starts at or before it).
+__device__ __forceinline__ int field_of_zseg(const FieldDev *f, int n, long long it)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (f[mid].zbase <= it) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Reconstruction for the z sweep with a warp-staged segment: a work item is
+// one warp's 32 consecutive interfaces along z of one (j, i) line.  The lanes
+// load the 37 cells the segment's stencils span (one coalesced load per lane
+// and component, five lanes load the upper halo), compute each cell's
+// temperature once and stage cells and temperatures in the warp's own
+// shared-memory tile; each lane then reads its six-cell stencil from there.
+// ---------------------------------------------------------------------------
+constexpr int kZSegWarps = kReconBlock / 32, kZSegCells = 32 + 5;
+
+template <int PREC, int MINB>
+__global__ void __launch_bounds__(kReconBlock, MINB) k_recon_zseg(Batch b)
+{
+    __shared__ double tiles[kZSegWarps][6][kZSegCells];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double (*tile)[kZSegCells] = tiles[wid];
+    const long long stride = (long long)gridDim.x * kZSegWarps;
+    for (long long it = (long long)blockIdx.x * kZSegWarps + wid; it < b.ztotal; it += stride) {
+        const FieldDev &f = b.fields[field_of_zseg(b.fields, b.nfields, it)];
+        const long long loc = it - f.zbase; // < nzseg: segment ranges are contiguous
+        const int nc = f.nc, nseg = (nc + 31) >> 5;
+        const long long line = loc / nseg;
+        const int k0 = int(loc - line * nseg) << 5;
+        const unsigned lbase = unsigned(line) * unsigned(nc); // cell (j, i, 0)
+        const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
+        // stage cells k0-2 .. k0+34 (those the active lanes' stencils reach:
+        // k0-2 .. min(k0+34, nc+2), so each index wraps at most once) and their
+        // temperatures
+        const int nh = min(kZSegCells, nc - k0 + 5);
+        for (int h = lane; h < nh; h += 32) {
+            const unsigned c = lbase + unsigned(wrap(k0 - 2 + h, nc));
+            double w[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                w[q] = __ldg(f.W[q] + c);
+                tile[q][h] = w[q];
+            }
+            tile[5][h] = direct ? 0.0 : temperature(w, f.cT);
+        }
+        __syncwarp();
+        const int k = k0 + lane;
+        if (k < nc) {
+            double s[6][5], T[6];
+#pragma unroll
+            for (int a = 0; a < 6; ++a) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) s[a][q] = tile[q][lane + a];
+                T[a] = tile[5][lane + a];
+            }
+            double wl[5], wr[5];
+            recon_point<PREC>(s, T, direct, f.icT, wl, wr);
+            const unsigned c = lbase + unsigned(k);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                f.rec[q][c] = wl[q];
+                f.rec[5 + q][c] = wr[q];
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Field of window item `it` (the last field whose window range starts at or before it).
 __device__ __forceinline__ int field_of_win(const FieldDev *f, int n, long long it)
 {
@@ -846,9 +920,9 @@ cudaError_t occ(KernelT k, int block, int *n)
 constexpr int kReconMinb[3] = {2, 3, 4};
 constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
 
-// Reconstruction variants: 0-2 the windowed kernel (x, y sweeps) at the three
-// register caps, 3-5 the one-interface-per-thread kernel at the same caps (the
-// z sweep always runs the latter).
+// Reconstruction variants: 0-2 the windowed kernel (x, y sweeps) or the
+// warp-staged segment kernel (z sweep) at the three register caps, 3-5 the
+// one-interface-per-thread kernel at the same caps.
 template <int DIR, int PREC>
 cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
 {
@@ -857,6 +931,12 @@ cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
         case 1: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
         case 2: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
         default: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        }
+    } else if (DIR == 2 && cfg.variant < 3) {
+        switch (cfg.variant) {
+        case 1: k_recon_zseg<PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon_zseg<PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        default: k_recon_zseg<PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
         }
     } else {
         switch (cfg.variant % 3) {
@@ -887,6 +967,11 @@ cudaError_t occ_kind(int kind, int variant, int block, int *n)
         if (variant == 1) return occ(k_recon_win<D, PREC, kReconMinb[1]>, block, n);
         if (variant == 2) return occ(k_recon_win<D, PREC, kReconMinb[2]>, block, n);
         return occ(k_recon_win<D, PREC, kReconMinb[0]>, block, n);
+    }
+    if (kind == K_RECON && DIR == 2 && variant < 3) {
+        if (variant == 1) return occ(k_recon_zseg<PREC, kReconMinb[1]>, block, n);
+        if (variant == 2) return occ(k_recon_zseg<PREC, kReconMinb[2]>, block, n);
+        return occ(k_recon_zseg<PREC, kReconMinb[0]>, block, n);
     }
     if (kind == K_RECON) {
         if (variant % 3 == 1) return occ(k_recon<DIR, PREC, kReconMinb[1]>, block, n);

@@ -26,6 +26,8 @@ struct FieldDev {
     long long nwin;   // window items: nc^2 * nrun
     int run;          // interfaces per window item (the same for every field of a batch)
     int nrun;         // runs per line: ceil(nc / run)
+    long long zbase;  // first z-segment item of this field (z reconstruction; one warp per item)
+    long long nzseg;  // z segments: nc^2 * ceil(nc / 32)
     int nc;
     unsigned nc_magic; // x / nc == (umulhi(x, nc_magic) + x) >> nc_shift for 32-bit x
     int nc_shift;
@@ -56,6 +58,7 @@ struct Batch {
     int nfields;
     long long total;  // end of the last field's item range
     long long wtotal; // end of the last field's window item range
+    long long ztotal; // end of the last field's z-segment item range
     int *err;         // device error word (bit 0: non-finite / non-positive state after update)
 };
 
