@@ -481,12 +481,11 @@ int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
     CK(cudaSetDevice(ctx->device));
     const FieldDev &d = ctx->fh[f].dev;
     CK(gks::launch_stats(d, d.F[0], ctx->d_partial, ctx->d_sums, ctx->stream));
-    double s[21];
+    double s[24];
     CK(cudaMemcpyAsync(s, ctx->d_sums, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     const gks_phys &p = ctx->fh[f].phys;
-    const double Nc = (double)d.ncell;
-    // PrintStats normalisation (update.cpp:727-776); s[0..17] are means already
+    // PrintStats normalisation (update.cpp:727-776); s[0..23] are means already
     out->tke = s[0];
     out->diss = s[1];
     out->sijsij = s[2];
@@ -496,9 +495,11 @@ int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
     out->kurt[0] = s[5] / (s[3] * s[3]);
     out->kurt[1] = s[8] / (s[6] * s[6]);
     out->kurt[2] = s[11] / (s[9] * s[9]);
-    out->prms = std::sqrt(s[18] / Nc) / (p.gam * p.p0 * p.Mt * p.Mt);
-    out->trms = std::sqrt(s[19] / Nc) / ((p.gam - 1) * p.T0 * p.Mt * p.Mt);
-    out->vrms = std::sqrt(s[20] / Nc) / (p.Mt * p.Mt / p.den0);
+    // population variances from the shifted moments: E[(x-K)^2] - E[x-K]^2
+    auto var = [&](int i) { return std::max(0.0, s[i + 1] - s[i] * s[i]); };
+    out->prms = std::sqrt(var(18)) / (p.gam * p.p0 * p.Mt * p.Mt);
+    out->trms = std::sqrt(var(20)) / ((p.gam - 1) * p.T0 * p.Mt * p.Mt);
+    out->vrms = std::sqrt(var(22)) / (p.Mt * p.Mt / p.den0);
     out->mach_t = std::sqrt(s[15]) / s[16];
     out->rho_mean = s[17];
     return GKS_OK;

@@ -644,65 +644,137 @@ __global__ void k_velocity(FieldDev f, double *scr)
 // padded block), for the three velocity components in turn:
 //   2 m0 + m1 = s (f1 - f0);  m_{p-1} + 4 m_p + m_{p+1} = s (f_{p+1} - f_{p-1});
 //   m_{n-2} + 2 m_{n-1} = s (f_{n-1} - f_{n-2}),  s = 3/h,
-// solved per line by the Thomas algorithm with precomputed pivots.  One warp
-// owns 32 lines, one lane per line.  Values move through a per-warp shared
-// tile 32 nodes at a time, so that every global access is a coalesced row
-// (along the line for axis 2, across lines otherwise) and a chunk's loads are
-// all in flight together instead of one dependent load per node.  Forward
-// values of interior nodes are parked in the output array and turned into
-// slopes by the backward pass.
-constexpr int kSplLines = 32, kSplChunk = 32, kSplPitch = kSplChunk + 3, kSplWarps = 4;
+// solved per line by the Thomas algorithm with precomputed pivots: forward
+// d_p = (r_p - d_{p-1}) inv_p, backward m_p = d_p - cp_p m_{p+1}, m_{nt-1} = d_{nt-1}.
+// One warp owns 32 lines, one lane per line.
+constexpr int kSplLines = 32, kSplChunk = 32, kSplPitch = kSplChunk + 3;
 
-__global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *scr, int axis)
+// x and y lines (k_spline_stream), one pass per line: the backward recurrence
+// forgets its start by a factor cp_p (-> 2 - sqrt 3 = 0.268) per node, so m_p
+// computed from m = 0 placed kSplTail = 32 nodes above p differs from the
+// exact slope by less than 0.27^32 ~ 5e-19 of the line's largest slope, far
+// below double rounding.  A lane runs the forward recurrence once along its
+// line, keeps the last kSplRing = 64 forward values in its column of a
+// shared-memory ring, and every 32 nodes runs the backward recurrence over
+// the ring, finalising the nodes that have 32 newer ones above them (at the
+// line's end, where m_{nt-1} = d_{nt-1} is exact, all the rest).  Each
+// velocity value is read once and each slope written once; consecutive lanes
+// own neighbouring lines, so every access is a coalesced row.
+constexpr int kSplRing = 64, kSplTail = 32, kSplRingPitch = kSplLines + 1;
+constexpr int kSplStreamWarps = 2; // 2 x 16.9 KB of ring per block
+// z lines (k_spline_tiled) are contiguous along the line, so a lane-per-line
+// access is a 32-way strided one; they take two passes (forward values
+// parked in the slope array, then the exact backward recurrence) through a
+// per-warp tile that turns every global access into a coalesced row.  The
+// streaming form needs ring and tile together, which at this shared-memory
+// footprint per warp halves the resident warps and measured 2.2x slower.
+constexpr int kSplTiledWarps = 4; // 4 x 9 KB of tile per block
+
+__global__ void __launch_bounds__(32 * kSplStreamWarps) k_spline_stream(FieldDev f, double *scr, int axis)
 {
-    __shared__ double tiles[kSplWarps][kSplLines][kSplPitch];
+    constexpr int NW = kSplStreamWarps;
+    __shared__ double rings[NW][kSplRing][kSplRingPitch];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double (*tile)[kSplPitch] = tiles[wid];
+    double (*ring)[kSplRingPitch] = rings[wid];
     const int nc = f.nc, nt = nc + 6;
     const long long n = f.ncell;
     const long long lines = (long long)nc * nc;
-    const long long line0 = ((long long)blockIdx.x * kSplWarps + wid) * kSplLines;
+    const long long line0 = ((long long)blockIdx.x * NW + wid) * kSplLines;
     if (line0 >= lines) return; // uniform per warp
     const int nl = int(min((long long)kSplLines, lines - line0));
-    const long long st = axis == 0 ? (long long)nc * nc : (axis == 1 ? (long long)nc : 1LL);
+    const long long st = axis == 0 ? (long long)nc * nc : (long long)nc;
     const bool mine = lane < nl;
-    // first cell of this lane's line: (i,k), (j,k) or (j,i) lines for axis 0, 1, 2;
-    // a lane reads another line's base with a shuffle
+    // first cell of this lane's line: (i,k) lines for axis 0, (j,k) for axis 1
     long long mybase;
     {
         const long long L = line0 + (mine ? lane : 0);
         const long long a = L / nc, b = L - a * nc;
-        mybase = axis == 0 ? a * nc + b : (axis == 1 ? a * nc * nc + b : (a * nc + b) * nc);
+        mybase = axis == 0 ? a * nc + b : a * nc * nc + b;
     }
     const double s = f.spl_s;
     const double *cp = f.spl_cp, *inv = f.spl_inv;
     // node p of a line sits at cell wrap(p - 3) along the axis
     auto node_off = [&](int p) -> long long { return (long long)wrap(p - 3, nc) * st; };
-    // Every chunk's loads are issued before any of them is used (fully
-    // unrolled, predicated), so a chunk costs one memory latency, not one per node.
 
 #pragma unroll 1
     for (int comp = 0; comp < 3; ++comp) {
         const double *u = scr + comp * n;
         double *g = scr + (3 + 3 * comp + axis) * n;
+        double dp = 0.0;
+        int fin = 3; // next node to finalise (nodes 0..2 are ghosts)
+#pragma unroll 1
+        for (int p0 = 0; p0 < nt; p0 += kSplChunk) {
+            // chunk values v[jj] = node p0 - 1 + jj, jj = 0 .. 33, all loads in flight at once
+            double v[kSplChunk + 2];
+#pragma unroll
+            for (int jj = 0; jj < kSplChunk + 2; ++jj) {
+                const int p = p0 - 1 + jj;
+                v[jj] = (mine && p >= 0 && p < nt) ? __ldg(u + mybase + node_off(p)) : 0.0;
+            }
+            // forward recurrence over the chunk's nodes into the ring
+            const int cend = min(kSplChunk, nt - p0);
+#pragma unroll
+            for (int c = 0; c < kSplChunk; ++c) {
+                if (c < cend) {
+                    const int p = p0 + c, jj = c + 1;
+                    if (p == 0) {
+                        dp = (s * (v[jj + 1] - v[jj])) * inv[0];
+                    } else {
+                        const double r = p < nt - 1 ? s * (v[jj + 1] - v[jj - 1]) : s * (v[jj] - v[jj - 1]);
+                        dp = (r - dp) * inv[p];
+                    }
+                    ring[p & (kSplRing - 1)][lane] = dp;
+                }
+            }
+            // finalise: backward from the newest node over the ring; the span
+            // phi - fin stays below kSplRing, so no slot is read after reuse
+            const int phi = p0 + cend - 1;
+            const int last = min(phi == nt - 1 ? phi : phi - kSplTail, nt - 4); // last node to emit
+            if (last >= fin) {
+                double m = 0.0;
+                for (int p = phi; p >= fin; --p) {
+                    double *slot = &ring[p & (kSplRing - 1)][lane];
+                    m = *slot - cp[p] * m;
+                    if (p <= last && mine) g[mybase + (long long)(p - 3) * st] = m;
+                }
+                fin = last + 1;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(32 * kSplTiledWarps) k_spline_tiled(FieldDev f, double *scr)
+{
+    constexpr int NW = kSplTiledWarps;
+    __shared__ double tiles[NW][kSplLines][kSplPitch];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double (*tile)[kSplPitch] = tiles[wid];
+    const int nc = f.nc, nt = nc + 6;
+    const long long n = f.ncell;
+    const long long lines = (long long)nc * nc;
+    const long long line0 = ((long long)blockIdx.x * NW + wid) * kSplLines;
+    if (line0 >= lines) return; // uniform per warp
+    const int nl = int(min((long long)kSplLines, lines - line0));
+    const bool mine = lane < nl;
+    // first cell of this lane's (j,i) line; a lane reads another line's base with a shuffle
+    const long long mybase = (line0 + (mine ? lane : 0)) * nc;
+    const double s = f.spl_s;
+    const double *cp = f.spl_cp, *inv = f.spl_inv;
+
+#pragma unroll 1
+    for (int comp = 0; comp < 3; ++comp) {
+        const double *u = scr + comp * n;
+        double *g = scr + (3 + 3 * comp + 2) * n;
         double dp = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0; // d0..d2: forward values of the last three nodes
         // forward pass: tile column jj holds node p0 - 1 + jj, jj = 0 .. 33
 #pragma unroll 1
         for (int p0 = 0; p0 < nt; p0 += kSplChunk) {
-            if (axis == 2) {
 #pragma unroll
-                for (int l = 0; l < kSplLines; ++l) {
-                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                    const int p = p0 - 1 + lane;
-                    if (l < nl && p >= 0 && p < nt) tile[l][lane] = __ldg(u + b + node_off(p));
-                    if (lane < 2 && l < nl && p + 32 < nt) tile[l][lane + 32] = __ldg(u + b + node_off(p + 32));
-                }
-            } else if (mine) {
-#pragma unroll
-                for (int jj = 0; jj < kSplChunk + 2; ++jj) {
-                    const int p = p0 - 1 + jj;
-                    if (p >= 0 && p < nt) tile[lane][jj] = __ldg(u + mybase + node_off(p));
-                }
+            for (int l = 0; l < kSplLines; ++l) {
+                const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                const int p = p0 - 1 + lane;
+                if (l < nl && p >= 0 && p < nt) tile[l][lane] = __ldg(u + b + wrap(p - 3, nc));
+                if (lane < 2 && l < nl && p + 32 < nt) tile[l][lane + 32] = __ldg(u + b + wrap(p + 29, nc));
             }
             __syncwarp();
             if (mine) {
@@ -724,19 +796,11 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
             }
             __syncwarp();
             // park forward values of nodes 3 .. nt-4 at cell p - 3
-            if (axis == 2) {
-                const int p = p0 + lane;
+            const int p = p0 + lane;
 #pragma unroll
-                for (int l = 0; l < kSplLines; ++l) {
-                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                    if (l < nl && p >= 3 && p <= nt - 4) g[b + (long long)(p - 3)] = tile[l][lane];
-                }
-            } else if (mine) {
-#pragma unroll
-                for (int c = 0; c < kSplChunk; ++c) {
-                    const int p = p0 + c;
-                    if (p >= 3 && p <= nt - 4) g[mybase + (long long)(p - 3) * st] = tile[lane][c];
-                }
+            for (int l = 0; l < kSplLines; ++l) {
+                const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                if (l < nl && p >= 3 && p <= nt - 4) g[b + (long long)(p - 3)] = tile[l][lane];
             }
             __syncwarp();
         }
@@ -747,16 +811,10 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
 #pragma unroll 1
         for (int q0 = ((nc - 1) / kSplChunk) * kSplChunk; q0 >= 0; q0 -= kSplChunk) {
             const int cnt = min(kSplChunk, nc - q0);
-            if (axis == 2) {
 #pragma unroll
-                for (int l = 0; l < kSplLines; ++l) {
-                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                    if (l < nl && lane < cnt) tile[l][lane] = g[b + (long long)(q0 + lane)];
-                }
-            } else if (mine) {
-#pragma unroll
-                for (int c = 0; c < kSplChunk; ++c)
-                    if (c < cnt) tile[lane][c] = g[mybase + (long long)(q0 + c) * st];
+            for (int l = 0; l < kSplLines; ++l) {
+                const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                if (l < nl && lane < cnt) tile[l][lane] = g[b + (long long)(q0 + lane)];
             }
             __syncwarp();
             if (mine) {
@@ -766,23 +824,17 @@ __global__ void __launch_bounds__(32 * kSplWarps) k_spline(FieldDev f, double *s
                 }
             }
             __syncwarp();
-            if (axis == 2) {
 #pragma unroll
-                for (int l = 0; l < kSplLines; ++l) {
-                    const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                    if (l < nl && lane < cnt) g[b + (long long)(q0 + lane)] = tile[l][lane];
-                }
-            } else if (mine) {
-#pragma unroll
-                for (int c = 0; c < kSplChunk; ++c)
-                    if (c < cnt) g[mybase + (long long)(q0 + c) * st] = tile[lane][c];
+            for (int l = 0; l < kSplLines; ++l) {
+                const long long b = __shfl_sync(0xffffffffu, mybase, l);
+                if (l < nl && lane < cnt) g[b + (long long)(q0 + lane)] = tile[l][lane];
             }
             __syncwarp();
         }
     }
 }
 
-constexpr int NSUM1 = 18, NSUM2 = 3;
+constexpr int NSUM1 = 24;
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -824,12 +876,21 @@ __device__ __forceinline__ void cell_prim(const FieldDev &f, long long c, double
     T = P * ri * f.iR;
 }
 
+// One pass over the cells: the means PrintStats forms (update.cpp:659-712)
+// and, for the rms of p, T and 1/rho (update.cpp:751-762), the first two
+// moments of x - K with K the value at cell 0 (shifted one-pass variance,
+// well conditioned because K lies inside the field's range).
 __global__ void k_sums1(FieldDev f, const double *scr, double *partial)
 {
     const long long n = f.ncell;
     double acc[NSUM1];
 #pragma unroll
     for (int i = 0; i < NSUM1; ++i) acc[i] = 0.0;
+    double Kp, Kt, Kv;
+    {
+        double den, u, v, w;
+        cell_prim(f, 0, den, Kv, u, v, w, Kp, Kt);
+    }
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
         double den, ri, u, v, w, P, T;
@@ -854,24 +915,15 @@ __global__ void k_sums1(FieldDev f, const double *scr, double *partial)
         acc[15] += u * u + v * v + w * w;
         acc[16] += sqrt(f.gam * P * ri);
         acc[17] += den;
+        const double dP = P - Kp, dT = T - Kt, dV = ri - Kv;
+        acc[18] += dP;
+        acc[19] += dP * dP;
+        acc[20] += dT;
+        acc[21] += dT * dT;
+        acc[22] += dV;
+        acc[23] += dV * dV;
     }
     block_sums<NSUM1>(acc, partial + (long long)blockIdx.x * NSUM1);
-}
-
-__global__ void k_sums2(FieldDev f, const double *means, double *partial)
-{
-    const long long n = f.ncell;
-    const double Pm = means[12], Tm = means[13], Vm = means[14];
-    double acc[NSUM2] = {0.0, 0.0, 0.0};
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
-        double den, ri, u, v, w, P, T;
-        cell_prim(f, c, den, ri, u, v, w, P, T);
-        acc[0] += (Pm - P) * (Pm - P);
-        acc[1] += (Tm - T) * (Tm - T);
-        acc[2] += (Vm - ri) * (Vm - ri);
-    }
-    block_sums<NSUM2>(acc, partial + (long long)blockIdx.x * NSUM2);
 }
 
 // Sum the per-block partials, one warp per quantity, in a fixed order (so the
@@ -1041,14 +1093,12 @@ cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, do
     const int grid = std::min(grid_for(f.ncell, block), 148 * 8);
     k_velocity<<<grid, block, 0, st>>>(f, scratch);
     const long long lines = (long long)f.nc * f.nc;
-    const int lper = kSplLines * kSplWarps;
-    const int lgrid = int((lines + lper - 1) / lper);
-    for (int axis = 0; axis < 3; ++axis) k_spline<<<lgrid, 32 * kSplWarps, 0, st>>>(f, scratch, axis);
+    auto lgrid = [&](int nw) { return int((lines + kSplLines * nw - 1) / (kSplLines * nw)); };
+    for (int axis = 0; axis < 2; ++axis)
+        k_spline_stream<<<lgrid(kSplStreamWarps), 32 * kSplStreamWarps, 0, st>>>(f, scratch, axis);
+    k_spline_tiled<<<lgrid(kSplTiledWarps), 32 * kSplTiledWarps, 0, st>>>(f, scratch);
     k_sums1<<<grid, block, 0, st>>>(f, scratch, partial);
     k_finalize<<<1, 32 * NSUM1, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
-    double *partial2 = partial + (long long)grid * NSUM1;
-    k_sums2<<<grid, block, 0, st>>>(f, sums, partial2);
-    k_finalize<<<1, 32 * NSUM2, 0, st>>>(partial2, grid, NSUM2, 1.0, sums + NSUM1);
     return cudaGetLastError();
 }
 

@@ -95,8 +95,9 @@ cudaError_t launch_scatter(const FieldDev &f, double *stage, cudaStream_t st);
 // *out_bits must be zero on entry).
 cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, cudaStream_t st);
 
-// Statistics of one field.  scratch: 12 * nc^3 doubles; partial: >= 2 * 32 * nblocks doubles.
-// Writes 16 sums of the first pass and 3 of the second into sums[0..18].
+// Statistics of one field.  scratch: 12 * nc^3 doubles; partial: >= 24 * nblocks doubles.
+// Writes 24 means into sums[0..23]: the 18 PrintStats means and, for p, T and
+// 1/rho, the means of x - K and (x - K)^2 (K = the value at cell 0).
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, cudaStream_t st);
 
 // Scan a field for non-finite values or non-positive density / pressure; sets bit 1 of *err.
