@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "gks_erfcx.cuh"
+
 namespace gks {
 
 constexpr double kPi = 3.141592653589793;  // atan(1)*4, param.h:14
@@ -107,6 +109,23 @@ __device__ __forceinline__ void weno_pair(T LLL, T LL, T L, T R, T RR, T RRR, T 
     s = fmaT(m2, RR, R + RRR);  const T q3 = k13 * s * s;
     wl = weno_side<T>(LLL, LL, L, R, RR, RRR, q0, q1, q2, q3, eps);
     wr = weno_side<T>(RRR, RR, R, L, LL, LLL, q3, q2, q1, q0, eps);
+}
+
+// ---------------------------------------------------------------------------
+// Half-space seed 0.5 erfc(|x|) from ex = exp(-x^2), which the half-space
+// tables need anyway: erfc(a) = exp(-a^2) erfcx(a), erfcx evaluated as its
+// Chebyshev interpolant in t = (a - K)/(a + K) (gen_erfcx.py; relative error
+// below 5e-16 for a <= 6, 2e-15 up to the underflow of exp(-a^2)).  The other
+// half is 1 - 0.5 erfc(|x|), without cancellation.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double half_erfc_abs(double x, double ex)
+{
+    const double a = fabs(x);
+    const double t = (a - kErfcxK) * __drcp_rn(a + kErfcxK);
+    double p = kErfcxC[kErfcxDeg];
+#pragma unroll
+    for (int i = kErfcxDeg - 1; i >= 0; --i) p = fma(p, t, kErfcxC[i]);
+    return (0.5 * ex) * p;
 }
 
 // ---------------------------------------------------------------------------

@@ -204,8 +204,11 @@ __device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, 
     {
         // one reciprocal square root: sqrt(lambda) = lambda / sqrt(lambda)
         const double rl = rsqrt(g.lam), sl = g.lam * rl;
-        const double h0 = 0.5 * erfc(NEG ? sl * g.U0 : -sl * g.U0);
-        const double ex = exp(-g.lam * g.U0 * g.U0) * (kHalfRsqrtPi * rl);
+        const double x = NEG ? sl * g.U0 : -sl * g.U0; // h0 = 0.5 erfc(x)
+        const double e2 = exp(-g.lam * g.U0 * g.U0);
+        const double tail = half_erfc_abs(x, e2);
+        const double h0 = x >= 0.0 ? tail : 1.0 - tail;
+        const double ex = e2 * (kHalfRsqrtPi * rl);
         half_table<7>(g.U0, g.s, h0, NEG ? -ex : ex, Xh);
     }
     full_table<6, double>(g.U0, g.s, Xf);
@@ -471,8 +474,9 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         // directly, the other value as 1 - tail (no cancellation)
         const double rl = rsqrt(e.lam), sl = e.lam * rl;
         const double x = sl * e.U0;
-        const double tail = 0.5 * erfc(fabs(x));
-        const double g = exp(-e.lam * e.U0 * e.U0) * (kHalfRsqrtPi * rl);
+        const double e2 = exp(-e.lam * e.U0 * e.U0);
+        const double tail = half_erfc_abs(x, e2);
+        const double g = e2 * (kHalfRsqrtPi * rl);
         half_table<7>(e.U0, e.s, x >= 0.0 ? 1.0 - tail : tail, g, Xp);
         half_table<7>(e.U0, e.s, x >= 0.0 ? tail : 1.0 - tail, -g, Xn);
     }
