@@ -160,23 +160,36 @@ struct Prim {
     double den, rinv, U0, U1, U2, P, lam, s; // s = 1/(2 lambda) = P/den
 };
 
-__device__ __forceinline__ Prim prim(const double W[5], double gm1)
+// rho (rho E) - |m|^2 / 2 = rho^2 p / (gamma - 1): the pressure times rho^2 /
+// (gamma - 1), without a division.
+__device__ __forceinline__ double rho2p(const double W[5])
+{
+    return fma(-0.5, fma(W[1], W[1], fma(W[2], W[2], W[3] * W[3])), W[0] * W[4]);
+}
+
+// With A = rho2p(W) and one reciprocal r = 1 / (rho A): 1/rho = A r,
+// p = (gamma - 1) A / rho, lambda = rho / (2 p) = rho^2 (rho r) / (2 (gamma - 1));
+// hig = 1 / (2 (gamma - 1)).
+__device__ __forceinline__ Prim prim(const double W[5], double gm1, double hig)
 {
     Prim p;
     p.den = W[0];
-    p.rinv = rcp<double>(W[0]);
+    const double A = rho2p(W);
+    const double r = rcp<double>(W[0] * A);
+    p.rinv = A * r;
     p.U0 = W[1] * p.rinv;
     p.U1 = W[2] * p.rinv;
     p.U2 = W[3] * p.rinv;
-    p.P = gm1 * fma(-0.5, fma(W[1], p.U0, fma(W[2], p.U1, W[3] * p.U2)), W[4]);
+    p.P = gm1 * (A * p.rinv);
     p.s = p.P * p.rinv;
-    p.lam = 0.5 * p.den * rcp<double>(p.P);
+    p.lam = hig * (W[0] * W[0]) * (W[0] * r);
     return p;
 }
 
 // Constants of one field that the flux needs.
 struct FluxConst {
     double gm1;   // gamma - 1
+    double hig;   // 1 / (2 (gamma - 1))
     double dt, dx;
     double ks[3]; // slope scales: 2/dx (normal), +-1/(2 dx) (transverse)
     double kA;    // pr_factor * 4 / (K + 3)

@@ -200,7 +200,7 @@ __device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, 
     constexpr bool FIRST = NEG == 0;
     double W[5];
     src.state(NEG, W);
-    const Prim g = prim(W, c.gm1);
+    const Prim g = prim(W, c.gm1, c.hig);
     {
         // one reciprocal square root: sqrt(lambda) = lambda / sqrt(lambda)
         const double rl = rsqrt(g.lam), sl = g.lam * rl;
@@ -402,13 +402,6 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
     asm volatile("" ::: "memory");
 }
 
-// p = (gamma - 1)(E - |m|^2 / (2 rho)), as in prim().
-__device__ __forceinline__ double pressure(const double W[5], double gm1)
-{
-    const double ri = rcp<double>(W[0]);
-    return gm1 * fma(-0.5, fma(W[1], W[1] * ri, fma(W[2], W[2] * ri, W[3] * (W[3] * ri))), W[4]);
-}
-
 // Time-integrated BGK-NS flux through one interface, in the frame of the
 // interface normal.  `src` supplies the inputs when they are needed, so that
 // one side's inputs are not live while the other side is processed, and keeps
@@ -428,13 +421,15 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
     SideWeights tw;
     {
         // collision time with the pressure-jump term (GKMflux.cpp:149-150):
-        // rho/lambda = 2p, so w = |p_l - p_r| / (p_l + p_r)
+        // rho/lambda = 2p, so w = |p_l - p_r| / (p_l + p_r); with
+        // p = (gamma - 1) A / rho, A = rho2p(W), multiplied through by
+        // rho_l rho_r / (gamma - 1): w = |A_l rho_r - A_r rho_l| / (A_l rho_r + A_r rho_l)
         double W[5];
         src.state(0, W);
-        const double pl = pressure(W, c.gm1);
+        const double Al = rho2p(W), rl = W[0];
         src.state(1, W);
-        const double pr = pressure(W, c.gm1);
-        tau = fma(dt, fabs(pl - pr) * rcp<double>(pl + pr), tau0);
+        const double a = Al * W[0], b = rho2p(W) * rl;
+        tau = fma(dt, fabs(a - b) * rcp<double>(a + b), tau0);
         ex = exp(-dt * rcp<double>(tau));
         om = 1.0 - ex;
         // gamma weights (GKMflux.cpp:155-157) and time integrals (GKMflux.cpp:186-190)
@@ -466,7 +461,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
     double We[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) We[q] = src.get_d(q);
-    const Prim e = prim(We, c.gm1);
+    const Prim e = prim(We, c.gm1, c.hig);
     double Xf[6], Xp[7], Xn[7];
     full_table<6, double>(e.U0, e.s, Xf);
     {

@@ -77,6 +77,23 @@ __device__ __forceinline__ double viscosity(const FieldDev &f, double T)
     return f.mu0 * (x * sqrt(x)) * (f.T0 + 110.4) * __drcp_rn(T + 110.4);
 }
 
+// Collision time mu / p of the state W (update.cpp:262-264).  Sutherland,
+// with A = rho2p(W), T = cT A / rho^2 and p = (gamma - 1) A / rho:
+//   mu / p = mu0 y^1.5 (T0 + 110.4) / ((gamma - 1) A (cT A + 110.4 rho^2)),  y = cT A / T0,
+// in which the powers of rho cancel: one reciprocal and one square root.
+__device__ __forceinline__ double visc_over_p(const FieldDev &f, const double W[5])
+{
+    const double A = rho2p(W);
+    if (f.visc_law == GKS_VISC_POWER) {
+        const double ri = __drcp_rn(W[0]);
+        const double P = f.gm1 * (A * ri);
+        return viscosity(f, P * ri * f.iR) * __drcp_rn(P);
+    }
+    const double y = (f.cT * A) * f.iT0;
+    const double den = (f.gm1 * A) * fma(110.4 * W[0], W[0], f.cT * A);
+    return (f.mu0 * (y * sqrt(y))) * (f.T0 + 110.4) * __drcp_rn(den);
+}
+
 __device__ __forceinline__ double temperature(const double W[5], double cT)
 {
     // (gam-1)(E/rho - |m|^2/(2 rho^2))/R, update.cpp:560
@@ -532,13 +549,11 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
             double w[5];
 #pragma unroll
             for (int q = 0; q < 5; ++q) w[SweepSrc<DIR, S>::perm(q)] = WL[q];
-            const double ri = __drcp_rn(w[0]);
-            const double P = f.gm1 * fma(-0.5 * fma(w[1], w[1], fma(w[2], w[2], w[3] * w[3])), ri, w[4]);
-            const double T = P * ri * f.iR;
-            tau0 = viscosity(f, T) * __drcp_rn(P);
+            tau0 = visc_over_p(f, w);
         }
         FluxConst fc;
         fc.gm1 = f.gm1;
+        fc.hig = 0.5 * (f.icT * f.iR); // R / (gamma - 1) * 1 / R
         fc.dt = f.dt;
         fc.dx = f.dx;
         fc.ks[0] = 2.0 * f.inv_dx;
