@@ -115,16 +115,16 @@ __device__ __forceinline__ double energy(const double w[5], double T, double ri,
 // stencil's temperatures T[0..5] (used unless GKS_DIRECT_ENERGY)
 // (update.cpp:247, 502-625 / GPUupdate.cu:917-977).
 // ---------------------------------------------------------------------------
-template <int PREC>
-__device__ __forceinline__ void recon_point(const double (&s)[6][5], const double (&T)[6], bool direct, double icT,
-                                            double wl[5], double wr[5])
+template <int PREC, typename SG>
+__device__ __forceinline__ void recon_point(const SG &s, const double (&T)[6], bool direct, double icT, double wl[5],
+                                            double wr[5])
 {
     if (PREC == 0) {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-            weno_pair<double>(s[0][q], s[1][q], s[2][q], s[3][q], s[4][q], s[5][q], kWenoEps, wl[q], wr[q]);
+            weno_pair<double>(s(0, q), s(1, q), s(2, q), s(3, q), s(4, q), s(5, q), kWenoEps, wl[q], wr[q]);
         if (direct) {
-            weno_pair<double>(s[0][4], s[1][4], s[2][4], s[3][4], s[4][4], s[5][4], kWenoEps, wl[4], wr[4]);
+            weno_pair<double>(s(0, 4), s(1, 4), s(2, 4), s(3, 4), s(4, 4), s(5, 4), kWenoEps, wl[4], wr[4]);
         } else {
             double tl, tr;
             weno_pair<double>(T[0], T[1], T[2], T[3], T[4], T[5], kWenoEps, tl, tr);
@@ -140,10 +140,10 @@ __device__ __forceinline__ void recon_point(const double (&s)[6][5], const doubl
         const float epsf = float(kWenoEps);
 #pragma unroll
         for (int q = 0; q < 4; q += 2) {
-            const double c0 = s[2][q], c1 = s[2][q + 1];
+            const double c0 = s(2, q), c1 = s(2, q + 1);
             f2 v[6];
 #pragma unroll
-            for (int a = 0; a < 6; ++a) v[a] = f2(float(s[a][q] - c0), float(s[a][q + 1] - c1));
+            for (int a = 0; a < 6; ++a) v[a] = f2(float(s(a, q) - c0), float(s(a, q + 1) - c1));
             f2 dl, dr;
             weno_pair<f2>(v[0], v[1], f2(0.0f), v[3], v[4], v[5], f2(epsf), dl, dr);
             wl[q] = c0 + double(dl.v.x);
@@ -152,10 +152,10 @@ __device__ __forceinline__ void recon_point(const double (&s)[6][5], const doubl
             wr[q + 1] = c1 + double(dr.v.y);
         }
         if (direct) {
-            const double c0 = s[2][4];
+            const double c0 = s(2, 4);
             float dl, dr;
-            weno_pair<float>(float(s[0][4] - c0), float(s[1][4] - c0), 0.0f, float(s[3][4] - c0),
-                             float(s[4][4] - c0), float(s[5][4] - c0), epsf, dl, dr);
+            weno_pair<float>(float(s(0, 4) - c0), float(s(1, 4) - c0), 0.0f, float(s(3, 4) - c0),
+                             float(s(4, 4) - c0), float(s(5, 4) - c0), epsf, dl, dr);
             wl[4] = c0 + double(dl);
             wr[4] = c0 + double(dr);
         } else {
@@ -168,6 +168,19 @@ __device__ __forceinline__ void recon_point(const double (&s)[6][5], const doubl
             wr[4] = energy(wr, tr, ir, icT);
         }
     }
+}
+
+// The stencil as a 6 x 5 array in registers.
+struct StencilRegs {
+    const double (&v)[6][5];
+    __device__ double operator()(int a, int q) const { return v[a][q]; }
+};
+
+template <int PREC>
+__device__ __forceinline__ void recon_point(const double (&s)[6][5], const double (&T)[6], bool direct, double icT,
+                                            double wl[5], double wr[5])
+{
+    recon_point<PREC>(StencilRegs{s}, T, direct, icT, wl, wr);
 }
 
 // ---------------------------------------------------------------------------
@@ -298,19 +311,20 @@ __device__ __forceinline__ int field_of_win(const FieldDev *f, int n, long long 
 // Reconstruction for the x (DIR 0) and y (DIR 1) sweeps with a sliding
 // window: a work item is a run of f.run consecutive interfaces along the
 // sweep at one (transverse line, k); the lanes of a warp take consecutive
-// k, so every load is coalesced.  The six stencil cells and their
-// temperatures stay in registers and move by one cell per interface: one new
-// cell (five loads) and one temperature per interface instead of thirty loads
-// and six temperatures.  Item order: k fastest, then run, then the transverse
-// line.  The loop is kept rolled (FP64) or unrolled twice (mixed): a fully
-// unrolled run holds several interfaces' loads and WENO temporaries at once
-// and needs more than 255 registers in FP64.  The cells entering the window
-// are fetched kWinPrefetch interfaces ahead by asynchronous copies into the
-// thread's own shared-memory slots ([slot][component][thread]), so their
-// memory latency overlaps the WENO of the interfaces before them without
-// holding registers; each interface waits only for its own cell's copies.
+// k, so every load is coalesced.  The window moves by one cell per
+// interface: one new cell (five loads) and one temperature per interface
+// instead of thirty loads and six temperatures.  The cells live in a ring of
+// kWinRing slots in the thread's own part of shared memory
+// ([slot][component][thread], no bank conflicts) -- the six stencil cells and
+// the kWinPrefetch cells beyond them, which arrive by asynchronous copies so
+// that their latency overlaps the WENO of the interfaces before them -- and
+// only the six temperatures stay in registers (FP64 98, mixed 110 registers
+// instead of 136 and 148 with the window in registers).  Item order: k
+// fastest, then run, then the transverse line.  The loop is kept rolled
+// (FP64) or unrolled twice (mixed).
 // ---------------------------------------------------------------------------
-constexpr int kWinPrefetch = 2; // a power of two; 2, 4 and 8 measured within 1 %
+constexpr int kWinPrefetch = 2; // 2, 4 and 8 measured within 1 %
+constexpr int kWinRing = 8;     // ring slots per thread: 6 stencil cells + the cells in flight
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
 {
@@ -327,9 +341,9 @@ __device__ __forceinline__ void cp_async_wait()
 template <int DIR, int PREC, int MINB>
 __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
 {
-    constexpr int PF = kWinPrefetch;
-    static_assert(PF >= 1 && (PF & (PF - 1)) == 0, "prefetch depth is a power of two");
-    __shared__ double pf[PF][5][kReconBlock];
+    constexpr int PF = kWinPrefetch, NR = kWinRing;
+    static_assert(NR >= 5 + PF && (NR & (NR - 1)) == 0, "the ring holds the window and the cells in flight");
+    __shared__ double ring[NR][5][kReconBlock];
     const int tid = threadIdx.x;
     static_assert(DIR == 0 || DIR == 1, "windowed reconstruction is for the x and y sweeps");
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -350,54 +364,52 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
                                         : unsigned(line) * unsigned(nc) + unsigned(k);
         auto cell = [&](int p) -> unsigned { return lbase + unsigned(wrap(p, nc)) * step; };
         const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
-        // cells entering the window: s0 + 3 .. last (unwrapped, at most nc + 2)
+        // cells of the run's stencils: s0 - 2 .. last (unwrapped, at most nc + 2),
+        // cell pc in ring slot pc mod NR, one copy group per cell (empty past the run)
         const int last = min(s0 + RUN, nc) + 2;
         auto fetch = [&](int pc) {
             if (pc <= last) {
                 const unsigned c = cell(pc);
 #pragma unroll
-                for (int q = 0; q < 5; ++q) cp_async8(&pf[pc & (PF - 1)][q][tid], f.W[q] + c);
+                for (int q = 0; q < 5; ++q) cp_async8(&ring[pc & (NR - 1)][q][tid], f.W[q] + c);
             }
-            cp_async_commit(); // one group per cell, empty past the run
+            cp_async_commit();
+        };
+        auto temp_of = [&](int pc) -> double {
+            double w[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) w[q] = ring[pc & (NR - 1)][q][tid];
+            return temperature(w, f.cT);
         };
 #pragma unroll
-        for (int d = 0; d < PF; ++d) fetch(s0 + 3 + d);
-        double s[6][5], T[6];
+        for (int d = 0; d < 5 + PF; ++d) fetch(s0 - 2 + d);
+        cp_async_wait<PF>(); // the five first window cells have landed
+        double T[6];
 #pragma unroll
-        for (int a = 0; a < 5; ++a) {
-            const unsigned c = cell(s0 - 2 + a);
-#pragma unroll
-            for (int q = 0; q < 5; ++q) s[a + 1][q] = __ldg(f.W[q] + c);
-            T[a + 1] = direct ? 0.0 : temperature(s[a + 1], f.cT);
-        }
+        for (int a = 0; a < 5; ++a) T[a + 1] = direct ? 0.0 : temp_of(s0 - 2 + a);
         constexpr int UNROLL = PREC == 0 ? 1 : 2;
 #pragma unroll UNROLL
         for (int r = 0; r < RUN; ++r) {
             const int p = s0 + r;
             if (p >= nc) break;
-            // slide: cells p-2 .. p+2 move down one slot, cell p+3 enters slot 5
 #pragma unroll
-            for (int a = 0; a < 5; ++a) {
-#pragma unroll
-                for (int q = 0; q < 5; ++q) s[a][q] = s[a + 1][q];
-                T[a] = T[a + 1];
-            }
-            cp_async_wait<PF - 1>(); // the group of cell p + 3 (issued PF groups ago) has landed
-#pragma unroll
-            for (int q = 0; q < 5; ++q) s[5][q] = pf[(p + 3) & (PF - 1)][q][tid];
-            T[5] = direct ? 0.0 : temperature(s[5], f.cT);
+            for (int a = 0; a < 5; ++a) T[a] = T[a + 1];
+            cp_async_wait<PF - 1>(); // cell p + 3 (issued PF groups ago) has landed
+            T[5] = direct ? 0.0 : temp_of(p + 3);
+            const auto sg = [&](int a, int q) -> double { return ring[(p - 2 + a) & (NR - 1)][q][tid]; };
             double wl[5], wr[5];
-            recon_point<PREC>(s, T, direct, f.icT, wl, wr);
+            recon_point<PREC>(sg, T, direct, f.icT, wl, wr);
             const unsigned c = cell(p);
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 f.rec[q][c] = wl[q];
                 f.rec[5 + q][c] = wr[q];
             }
-            // the slot of cell p + 3 was read above; refill it with cell p + 3 + PF
+            // cell p + 3 + PF takes the slot of cell p + 3 + PF - NR, which no
+            // stencil from here on reads (it lies below p - 2 for NR >= 5 + PF)
             fetch(p + 3 + PF);
         }
-        cp_async_wait<0>(); // nothing in flight into the slots before the next item
+        cp_async_wait<0>(); // nothing in flight into the ring before the next item
     }
 }
 
@@ -1021,7 +1033,7 @@ cudaError_t occ(KernelT k, int block, int *n)
 // and the one-interface form, flux blocks of 64 threads at
 // 4 / 6 / 8 -> 255 / 168 / 128 registers); the tuner picks one per
 // kernel, precision and sweep.  Every variant gives bit-identical results.
-constexpr int kReconMinb[3] = {2, 3, 4};
+constexpr int kReconMinb[3] = {3, 4, 5};
 constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
 
 // Reconstruction variants: 0-2 the windowed kernel (x, y sweeps) or the
