@@ -241,6 +241,19 @@ __device__ __forceinline__ int field_of_zseg(const FieldDev *f, int n, long long
 // temperature once and stage cells and temperatures in the warp's own
 // shared-memory tile; each lane then reads its six-cell stencil from there.
 // ---------------------------------------------------------------------------
+// Asynchronous 8-byte copy global -> shared (cp.async), its groups and waits.
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
+{
+    const unsigned a = unsigned(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 constexpr int kZSegWarps = kReconBlock / 32, kZSegCells = 32 + 5;
 
 template <int PREC, int MINB>
@@ -260,17 +273,29 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_zseg(Batch b)
         const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
         // stage cells k0-2 .. k0+34 (those the active lanes' stencils reach:
         // k0-2 .. min(k0+34, nc+2), so each index wraps at most once) and their
-        // temperatures
+        // temperatures; lane l takes cells l and l + 32, all ten loads issued at once
         const int nh = min(kZSegCells, nc - k0 + 5);
-        for (int h = lane; h < nh; h += 32) {
-            const unsigned c = lbase + unsigned(wrap(k0 - 2 + h, nc));
-            double w[5];
+        const int h1 = lane + 32;
+        const bool one = lane < nh, two = h1 < nh;
+        double w[5], v[5];
+        {
+            const unsigned c0 = lbase + unsigned(wrap(k0 - 2 + (one ? lane : 0), nc));
+            const unsigned c1 = lbase + unsigned(wrap(k0 - 2 + (two ? h1 : 0), nc));
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                w[q] = __ldg(f.W[q] + c);
-                tile[q][h] = w[q];
+                w[q] = one ? __ldg(f.W[q] + c0) : 0.0;
+                v[q] = two ? __ldg(f.W[q] + c1) : 0.0;
             }
-            tile[5][h] = direct ? 0.0 : temperature(w, f.cT);
+        }
+        if (one) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) tile[q][lane] = w[q];
+            tile[5][lane] = direct ? 0.0 : temperature(w, f.cT);
+        }
+        if (two) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) tile[q][h1] = v[q];
+            tile[5][h1] = direct ? 0.0 : temperature(v, f.cT);
         }
         __syncwarp();
         const int k = k0 + lane;
@@ -326,17 +351,6 @@ __device__ __forceinline__ int field_of_win(const FieldDev *f, int n, long long 
 constexpr int kWinPrefetch = 2; // 2, 4 and 8 measured within 1 %
 constexpr int kWinRing = 8;     // ring slots per thread: 6 stencil cells + the cells in flight
 
-__device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
-{
-    const unsigned a = unsigned(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 template <int DIR, int PREC, int MINB>
 __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
