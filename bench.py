@@ -312,9 +312,12 @@ def run_accuracy(args):
     case = make_case(nc, 0, args.mach, args.re)
     W = gks_ic.to_conservative_padded(case)
     hist, ms = {}, {}
-    for name, prec in (("fp64", gks.FP64), ("mixed", gks.MIXED)):
+    # the control: a perturbation of FP32-rounding size in the initial field only
+    W32 = W.astype(np.float32).astype(np.float64) if args.control else None
+    runs = (("fp64", gks.FP64, W), ("mixed", gks.FP64 if args.control else gks.MIXED, W32 if args.control else W))
+    for name, prec, w0 in runs:
         with gks.Solver(gks.phys_from_case(case), prec) as s:
-            s.upload(W)
+            s.upload(w0)
             dt = s.timestep(CFL)
             nsteps = int(np.ceil(args.t_end * case.t0 / dt))
             h = []
@@ -329,7 +332,7 @@ def run_accuracy(args):
     keys = ("tke", "diss", "skew_u", "skew_v", "skew_w")
     final = {k: abs(hist["mixed"][-1][k] - hist["fp64"][-1][k]) / abs(hist["fp64"][-1][k]) for k in keys}
     worst = {k: max(abs(a[k] - b[k]) / abs(b[k]) for a, b in zip(hist["mixed"], hist["fp64"])) for k in keys}
-    print(json.dumps({"mode": "accuracy", "nc": nc, "mach_t": args.mach, "re_lambda": args.re,
+    print(json.dumps({"mode": "accuracy-control" if args.control else "accuracy", "nc": nc, "mach_t": args.mach, "re_lambda": args.re,
                       "t_over_t0": args.t_end, "steps": nsteps, "dt": dt,
                       "rel_err_final": final, "rel_err_max_over_history": worst,
                       "tke_fp64_initial": hist["fp64"][0]["tke"], "tke_fp64_final": hist["fp64"][-1]["tke"],
@@ -536,6 +539,8 @@ def main():
     ap.add_argument("--no-refgpu", action="store_true", help="skip timing the reference's own GPU path")
     ap.add_argument("--accuracy", action="store_true", help="mixed vs FP64 statistics to t/t0 = --t-end, then exit")
     ap.add_argument("--t-end", type=float, default=2.0, help="accuracy run length in eddy turnover times")
+    ap.add_argument("--control", action="store_true",
+                    help="with --accuracy: compare FP64 with FP64 started from the initial field rounded to FP32")
     ap.add_argument("--mach", type=float, default=MACH, help="turbulent Mach number of the field")
     ap.add_argument("--re", type=float, default=RE, help="Re_lambda of the field")
     args = ap.parse_args()
