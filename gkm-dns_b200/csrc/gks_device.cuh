@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 #include "gks_erfcx.cuh"
 
 namespace gks {
@@ -60,14 +62,16 @@ template <> __device__ __forceinline__ f2 cst<f2>(double x) { return f2(float(x)
 // WENO-SYMOO on one scalar 6-point stencil (update.cpp:505-557): four cubic
 // candidates per side, linear weights 1/20, 9/20, 9/20, 1/20, the fourth
 // smoothness indicator replaced by the largest of the four, alpha = g/(eps+IS).
-// The normalised weights are formed with one reciprocal per side:
+// The normalised weights are formed with one reciprocal per side (in double,
+// one for both sides of an interface, see weno_pair):
 // w_r = g_r prod_{s!=r} d_s / sum_t g_t prod_{s!=t} d_s, d = eps + IS.
 // ---------------------------------------------------------------------------
 // One side seen from (a, b, c | d, e, f): candidates on {a,b,c}, {b,c,d},
 // {c,d,e}, {d,e,f}; q0..q3 are 13/12 of the squared second differences of
 // those stencils, which both sides share.
 template <typename T>
-__device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1, T q2, T q3, T eps)
+__device__ __forceinline__ void weno_side_nd(T a, T b, T c, T d, T e, T f, T q0, T q1, T q2, T q3, T eps, T &num,
+                                             T &den)
 {
     const T third = cst<T>(1.0 / 3.0), msixth = cst<T>(-1.0 / 6.0);
     const T ms7 = cst<T>(-7.0 / 6.0), s11 = cst<T>(11.0 / 6.0), s5 = cst<T>(5.0 / 6.0);
@@ -92,8 +96,16 @@ __device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1,
     const T n1 = cst<T>(0.45) * (d0 * d23);
     const T n2 = cst<T>(0.45) * (d01 * d3);
     const T n3 = cst<T>(0.05) * (d01 * d2);
-    const T inv = rcp<T>(n0 + n1 + n2 + n3);
-    return fmaT(n0, p0, fmaT(n1, p1, fmaT(n2, p2, n3 * p3))) * inv;
+    den = n0 + n1 + n2 + n3;
+    num = fmaT(n0, p0, fmaT(n1, p1, fmaT(n2, p2, n3 * p3)));
+}
+
+template <typename T>
+__device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1, T q2, T q3, T eps)
+{
+    T num, den;
+    weno_side_nd<T>(a, b, c, d, e, f, q0, q1, q2, q3, eps, num, den);
+    return num * rcp<T>(den);
 }
 
 // Both interface values of the stencil (LLL, LL, L, R, RR, RRR): wl seen from
@@ -107,8 +119,20 @@ __device__ __forceinline__ void weno_pair(T LLL, T LL, T L, T R, T RR, T RRR, T 
     s = fmaT(m2, L, LL + R);    const T q1 = k13 * s * s;
     s = fmaT(m2, R, L + RR);    const T q2 = k13 * s * s;
     s = fmaT(m2, RR, R + RRR);  const T q3 = k13 * s * s;
-    wl = weno_side<T>(LLL, LL, L, R, RR, RRR, q0, q1, q2, q3, eps);
-    wr = weno_side<T>(RRR, RR, R, L, LL, LLL, q3, q2, q1, q0, eps);
+    if constexpr (std::is_same<T, double>::value) {
+        // double: one reciprocal for both sides, 1/Dl = Dr / (Dl Dr) (the
+        // normalisers lie between about 1e-30 and 1e9 with eps = 1e-10, so the
+        // product stays far inside the double range)
+        T nl, dl, nr, dr;
+        weno_side_nd<T>(LLL, LL, L, R, RR, RRR, q0, q1, q2, q3, eps, nl, dl);
+        weno_side_nd<T>(RRR, RR, R, L, LL, LLL, q3, q2, q1, q0, eps, nr, dr);
+        const T r = rcp<T>(dl * dr);
+        wl = nl * (dr * r);
+        wr = nr * (dl * r);
+    } else {
+        wl = weno_side<T>(LLL, LL, L, R, RR, RRR, q0, q1, q2, q3, eps);
+        wr = weno_side<T>(RRR, RR, R, L, LL, LLL, q3, q2, q1, q0, eps);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -129,9 +129,9 @@ __device__ __forceinline__ void recon_point(const SG &s, const double (&T)[6], b
             double tl, tr;
             weno_pair<double>(T[0], T[1], T[2], T[3], T[4], T[5], kWenoEps, tl, tr);
             // E from the reconstructed temperature (update.cpp:618-619)
-            const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
-            wl[4] = energy(wl, tl, il, icT);
-            wr[4] = energy(wr, tr, ir, icT);
+            const double r = __drcp_rn(wl[0] * wr[0]); // one reciprocal for both densities
+            wl[4] = energy(wl, tl, wr[0] * r, icT);
+            wr[4] = energy(wr, tr, wl[0] * r, icT);
         }
     } else {
         // mixed: WENO in FP32 on differences from the left cell, added back
@@ -163,9 +163,9 @@ __device__ __forceinline__ void recon_point(const SG &s, const double (&T)[6], b
             weno_pair<float>(float(T[0] - T[2]), float(T[1] - T[2]), 0.0f, float(T[3] - T[2]),
                              float(T[4] - T[2]), float(T[5] - T[2]), epsf, dl, dr);
             const double tl = T[2] + double(dl), tr = T[2] + double(dr);
-            const double il = __drcp_rn(wl[0]), ir = __drcp_rn(wr[0]);
-            wl[4] = energy(wl, tl, il, icT);
-            wr[4] = energy(wr, tr, ir, icT);
+            const double r = __drcp_rn(wl[0] * wr[0]); // one reciprocal for both densities
+            wl[4] = energy(wl, tl, wr[0] * r, icT);
+            wr[4] = energy(wr, tr, wl[0] * r, icT);
         }
     }
 }
