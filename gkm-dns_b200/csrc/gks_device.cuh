@@ -100,12 +100,25 @@ __device__ __forceinline__ void weno_side_nd(T a, T b, T c, T d, T e, T f, T q0,
     num = fmaT(n0, p0, fmaT(n1, p1, fmaT(n2, p2, n3 * p3)));
 }
 
+// Reciprocal of a WENO normaliser: correctly rounded in double; in FP32 the
+// hardware approximation (rcp.approx, within one unit in the last place), as
+// the weights only scale a difference from the centre cell and need FP32
+// accuracy, not rounding to nearest.
+template <typename T> __device__ __forceinline__ T rcp_weno(T x) { return rcp<T>(x); }
+template <> __device__ __forceinline__ float rcp_weno<float>(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+template <> __device__ __forceinline__ f2 rcp_weno<f2>(f2 x) { return f2(rcp_weno<float>(x.v.x), rcp_weno<float>(x.v.y)); }
+
 template <typename T>
 __device__ __forceinline__ T weno_side(T a, T b, T c, T d, T e, T f, T q0, T q1, T q2, T q3, T eps)
 {
     T num, den;
     weno_side_nd<T>(a, b, c, d, e, f, q0, q1, q2, q3, eps, num, den);
-    return num * rcp<T>(den);
+    return num * rcp_weno<T>(den);
 }
 
 // Both interface values of the stencil (LLL, LL, L, R, RR, RRR): wl seen from
