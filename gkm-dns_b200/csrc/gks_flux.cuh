@@ -412,9 +412,9 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
 //   src.put_d / put_s<FIRST>(slot, v), get_d / get_s(slot)   running sums
 // (the mixed path keeps its type-S sums in registers: the paired side pass
 // produces them all at once).
-// tau0 = mu/p at the left cell.  Output F[5], the flux integrated over [0, dt].
+// mu/p at the left cell = tau_n / tau_d.  Output F[5], the flux integrated over [0, dt].
 template <typename S, typename Src>
-__device__ __forceinline__ void gks_flux(const Src &src, double tau0, const FluxConst &c, double F[5])
+__device__ __forceinline__ void gks_flux(const Src &src, double tau_n, double tau_d, const FluxConst &c, double F[5])
 {
     const double dt = c.dt;
     double tau, ex, om, igm0;
@@ -429,8 +429,13 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau0, const Flux
         const double Al = rho2p(W), rl = W[0];
         src.state(1, W);
         const double a = Al * W[0], b = rho2p(W) * rl;
-        tau = fma(dt, fabs(a - b) * rcp<double>(a + b), tau0);
-        ex = exp(-dt * rcp<double>(tau));
+        // tau = tau_n / tau_d + dt w = N / D; one reciprocal r = 1 / (N D) gives
+        // tau = N (N r) and 1 / tau = D (D r)
+        const double D = tau_d * (a + b);
+        const double N = fma(tau_n, a + b, dt * fabs(a - b) * tau_d);
+        const double r = rcp<double>(N * D);
+        tau = N * (N * r);
+        ex = exp(-dt * (D * (D * r)));
         om = 1.0 - ex;
         // gamma weights (GKMflux.cpp:155-157) and time integrals (GKMflux.cpp:186-190)
         const double Pt = tau * om;

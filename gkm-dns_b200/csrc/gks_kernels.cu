@@ -77,21 +77,23 @@ __device__ __forceinline__ double viscosity(const FieldDev &f, double T)
     return f.mu0 * (x * sqrt(x)) * (f.T0 + 110.4) * __drcp_rn(T + 110.4);
 }
 
-// Collision time mu / p of the state W (update.cpp:262-264).  Sutherland,
-// with A = rho2p(W), T = cT A / rho^2 and p = (gamma - 1) A / rho:
+// Collision time mu / p of the state W (update.cpp:262-264) as a fraction
+// num / den, which the flux divides out together with its other terms.
+// Sutherland, with A = rho2p(W), T = cT A / rho^2 and p = (gamma - 1) A / rho:
 //   mu / p = mu0 y^1.5 (T0 + 110.4) / ((gamma - 1) A (cT A + 110.4 rho^2)),  y = cT A / T0,
-// in which the powers of rho cancel: one reciprocal and one square root.
-__device__ __forceinline__ double visc_over_p(const FieldDev &f, const double W[5])
+// in which the powers of rho cancel (no reciprocal at all).
+__device__ __forceinline__ void visc_over_p(const FieldDev &f, const double W[5], double &num, double &den)
 {
     const double A = rho2p(W);
     if (f.visc_law == GKS_VISC_POWER) {
         const double ri = __drcp_rn(W[0]);
-        const double P = f.gm1 * (A * ri);
-        return viscosity(f, P * ri * f.iR) * __drcp_rn(P);
+        den = f.gm1 * (A * ri);
+        num = viscosity(f, den * ri * f.iR);
+        return;
     }
     const double y = (f.cT * A) * f.iT0;
-    const double den = (f.gm1 * A) * fma(110.4 * W[0], W[0], f.cT * A);
-    return (f.mu0 * (y * sqrt(y))) * (f.T0 + 110.4) * __drcp_rn(den);
+    den = (f.gm1 * A) * fma(110.4 * W[0], W[0], f.cT * A);
+    num = (f.mu0 * (y * sqrt(y))) * (f.T0 + 110.4);
 }
 
 __device__ __forceinline__ double temperature(const double W[5], double cT)
@@ -568,14 +570,14 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
         src.sum_s = sum_s;
         src.load(f, x.c, along<DIR>(x, 1), cn, cs, cf, cb);
         // collision time at the left cell, in the unrotated frame (update.cpp:262-264)
-        double tau0;
+        double tau_n, tau_d; // mu / p = tau_n / tau_d
         {
             double WL[5], WR[5];
             src.cells(WL, WR);
             double w[5];
 #pragma unroll
             for (int q = 0; q < 5; ++q) w[SweepSrc<DIR, S>::perm(q)] = WL[q];
-            tau0 = visc_over_p(f, w);
+            visc_over_p(f, w, tau_n, tau_d);
         }
         FluxConst fc;
         fc.gm1 = f.gm1;
@@ -588,7 +590,7 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
         fc.kA = f.kA;
         fc.K = f.K;
         double F[5];
-        gks_flux<S>(src, tau0, fc, F);
+        gks_flux<S>(src, tau_n, tau_d, fc, F);
         constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
         if (ROT) {
             const double t = F[1];
