@@ -612,21 +612,25 @@ int gks_autotune(gks_ctx *ctx, int reps)
     for (int dir = 0; dir < 3 && rc == GKS_OK; ++dir) {
         for (int kind : {int(gks::K_RECON), int(gks::K_FLUX)}) {
             const int nvar = kind == gks::K_RECON ? gks::kReconVariants : gks::kFluxVariants;
-            float best = 1e30f;
-            gks::LaunchCfg bestc = ctx->cfg[kind][dir];
-            for (int v = 0; v < nvar && rc == GKS_OK; ++v)
-                for (int m : mults) {
-                    const gks::LaunchCfg c = persistent(ctx, kind, dir, v, m);
+            // every candidate is timed in two interleaved rounds and keeps its
+            // faster one, so that one disturbed measurement does not decide
+            std::vector<gks::LaunchCfg> cand;
+            for (int v = 0; v < nvar; ++v)
+                for (int m : mults) cand.push_back(persistent(ctx, kind, dir, v, m));
+            std::vector<float> t(cand.size(), 1e30f);
+            for (int round = 0; round < 2 && rc == GKS_OK; ++round)
+                for (size_t i = 0; i < cand.size() && rc == GKS_OK; ++i) {
                     float ms = 0;
-                    const cudaError_t e = time_it(kind, dir, c, &ms);
-                    if (e != cudaSuccess) {
-                        rc = cuda_fail(ctx, e, "autotune");
-                        break;
-                    }
-                    if (ms < best) {
-                        best = ms;
-                        bestc = c;
-                    }
+                    const cudaError_t e = time_it(kind, dir, cand[i], &ms);
+                    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "autotune");
+                    else if (ms < t[i]) t[i] = ms;
+                }
+            gks::LaunchCfg bestc = ctx->cfg[kind][dir];
+            float best = 1e30f;
+            for (size_t i = 0; i < cand.size(); ++i)
+                if (t[i] < best) {
+                    best = t[i];
+                    bestc = cand[i];
                 }
             ctx->cfg[kind][dir] = bestc;
             // leave this sweep's reconstruction in place for timing its flux
