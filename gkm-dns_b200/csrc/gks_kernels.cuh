@@ -46,10 +46,10 @@ struct FieldDev {
 constexpr int kItemAlign = 256;
 
 // Longest run of interfaces per work item of the windowed x / y
-// reconstruction (prec 0 FP64, 1 mixed; the lengths measured fastest on B200
-// at 256^3).  A batch halves it, down to kWinRunMin, while it has fewer than
+// reconstruction, for either precision (0 FP64, 1 mixed; 64 measured fastest
+// on B200 at 256^3 for both).  A batch halves it, down to kWinRunMin, while it has fewer than
 // kWinItemsPerSm items per SM, so that small fields still fill the GPU.
-__host__ __device__ constexpr int win_run(int prec) { return prec == 0 ? 64 : 32; }
+__host__ __device__ constexpr int win_run(int) { return 64; }
 constexpr int kWinRunMin = 8;
 constexpr int kWinItemsPerSm = 768;
 
