@@ -382,9 +382,22 @@ def run_ours(args):
     phys = gks.phys_from_case(case)
     uuid = gpu_uuid(local)
 
-    # peaks of the FP64 / FP32 pipes, measured here (no FP64 figure is supplied)
-    peak64 = gks.peak_tflops(gks.FP64)
+    # peaks of the FP64 / FP32 pipes, measured here (no FP64 figure is supplied):
+    # a first short burst, then the probe repeated for about 1.5 s, whose
+    # settled rate (median of the second half) is the sustained peak that a
+    # kernel timed inside the long step loop is compared with
+    peak64_burst = gks.peak_tflops(gks.FP64)
+    runs, t0 = [], time.perf_counter()
+    while time.perf_counter() - t0 < 1.5:
+        runs.append(gks.peak_tflops(gks.FP64))
+    peak64 = statistics.median(runs[len(runs) // 2:])
     peak32 = gks.peak_tflops(gks.MIXED)
+    hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            hbm_peak, hbm_src = float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
 
     results = {}
     solvers = {}
@@ -500,13 +513,16 @@ def run_ours(args):
                       "stage_ms": stages["mixed"]},
             "roofline": {"bound": "fp64", "kernel": "flux sweep (k_flux, FP64)", "achieved": achieved,
                          "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": traffic,
-                         "peak_source": "FP64 FMA peak measured live by gks_peak_flops on this GPU",
+                         "peak_source": "FP64 FMA peak measured live by gks_peak_flops on this GPU, sustained"
+                                        " (the probe repeated for 1.5 s; the kernel is timed inside the step loop)",
+                         "peak_burst": peak64_burst,
                          "ops_per_interface": OPS_FLUX, "launch_ms": flux_ms,
                          "fp64_pipe": fp64_pipe,
                          "step_achieved": OPS_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e12,
                          "fp32_peak": peak32},
             "hbm": {"achieved_gbs": BYTES_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e9,
-                    "peak_gbs": 6538.0, "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
+                    "peak_gbs": hbm_peak, "peak_source": hbm_src,
+                    "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
             "stage_ms": stages["fp64"], "recon_ms": recon_ms, "stats_ms": stats_ms,
             "ensemble": ens,
             "launch": {"fp64": results["fp64"]["launch"], "mixed": results["mixed"]["launch"],
