@@ -345,8 +345,8 @@ __device__ __forceinline__ int field_of_win(const FieldDev *f, int n, long long 
 // ([slot][component][thread], no bank conflicts) -- the six stencil cells and
 // the kWinPrefetch cells beyond them, which arrive by asynchronous copies so
 // that their latency overlaps the WENO of the interfaces before them -- and
-// only the six temperatures stay in registers (FP64 98, mixed 110 registers
-// instead of 136 and 148 with the window in registers).  Item order: k
+// only the six temperatures stay in registers (about 40 fewer registers than
+// with the window in registers).  Item order: k
 // fastest, then run, then the transverse line.  The loop is kept rolled
 // (FP64) or unrolled twice (mixed).
 // ---------------------------------------------------------------------------
@@ -1045,7 +1045,7 @@ cudaError_t occ(KernelT k, int block, int *n)
 }
 
 // Register-cap variants (min resident blocks per SM: reconstruction blocks of
-// 128 threads at 2 / 3 / 4 -> 255 / 168 / 128 registers, each in the windowed
+// 128 threads at 3 / 4 / 5 -> 168 / 128 / 96 registers, each in the windowed
 // and the one-interface form, flux blocks of 64 threads at
 // 4 / 6 / 8 -> 255 / 168 / 128 registers); the tuner picks one per
 // kernel, precision and sweep.  Every variant gives bit-identical results.
