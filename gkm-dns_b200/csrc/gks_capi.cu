@@ -1,7 +1,7 @@
 // C ABI of the WENO-GKS step (declarations in include/gks_b200.h).
 //
-// A context owns, per field, one device allocation of 30 * nc^3 doubles
-// (state 5, reconstruction 10, fluxes 15; the statistics reuse the flux
+// A context owns, per field, one device allocation of 32 * nc^3 doubles
+// (state 5, reconstruction 10, fluxes 15, mu/p 2; the statistics reuse the flux
 // arrays as scratch), the field's descriptor in a device array, and one
 // CUDA graph holding a whole step for all fields (seven persistent launches).
 // The reference instead allocates 50 padded arrays per rank and copies the
@@ -265,13 +265,14 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         h.phys = phys[f];
         const gks_phys &p = phys[f];
         const long long n = (long long)p.nc * p.nc * p.nc;
-        if (cudaMalloc(&h.mem, (size_t)30 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
-        cudaMemset(h.mem, 0, (size_t)30 * n * sizeof(double));
+        if (cudaMalloc(&h.mem, (size_t)32 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+        cudaMemset(h.mem, 0, (size_t)32 * n * sizeof(double));
         FieldDev &d = h.dev;
         memset(&d, 0, sizeof(d));
         for (int q = 0; q < 5; ++q) d.W[q] = h.mem + q * n;
         for (int q = 0; q < 10; ++q) d.rec[q] = h.mem + (5 + q) * n;
         for (int q = 0; q < 15; ++q) d.F[q] = h.mem + (15 + q) * n;
+        for (int q = 0; q < 2; ++q) d.tau[q] = h.mem + (30 + q) * n;
         const int nt = p.nc + 6;
         std::vector<double> cp, inv;
         spline_coeffs(nt, cp, inv);

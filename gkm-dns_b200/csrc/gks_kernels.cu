@@ -96,6 +96,16 @@ __device__ __forceinline__ void visc_over_p(const FieldDev &f, const double W[5]
     num = (f.mu0 * (y * sqrt(y))) * (f.T0 + 110.4);
 }
 
+// mu/p of cell c, stored once per step by the x-sweep reconstruction for the
+// flux kernels of all three sweeps (the left cell of interface c is c in each).
+__device__ __forceinline__ void store_tau(const FieldDev &f, unsigned c, const double W[5])
+{
+    double n, d;
+    visc_over_p(f, W, n, d);
+    f.tau[0][c] = n;
+    f.tau[1][c] = d;
+}
+
 __device__ __forceinline__ double temperature(const double W[5], double cT)
 {
     // (gam-1)(E/rho - |m|^2/(2 rho^2))/R, update.cpp:560
@@ -207,6 +217,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
         for (int a = 0; a < 6; ++a)
 #pragma unroll
             for (int q = 0; q < 5; ++q) s[a][q] = __ldg(f.W[q] + idx[a]);
+        if (DIR == 0) store_tau(f, x.c, s[2]);
         const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
         double T[6];
         if (!direct) {
@@ -416,6 +427,12 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
             double wl[5], wr[5];
             recon_point<PREC>(sg, T, direct, f.icT, wl, wr);
             const unsigned c = cell(p);
+            if (DIR == 0) {
+                double w[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) w[q] = sg(2, q);
+                store_tau(f, c, w);
+            }
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 f.rec[q][c] = wl[q];
@@ -569,16 +586,9 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
         src.sum_d = sum_d;
         src.sum_s = sum_s;
         src.load(f, x.c, along<DIR>(x, 1), cn, cs, cf, cb);
-        // collision time at the left cell, in the unrotated frame (update.cpp:262-264)
-        double tau_n, tau_d; // mu / p = tau_n / tau_d
-        {
-            double WL[5], WR[5];
-            src.cells(WL, WR);
-            double w[5];
-#pragma unroll
-            for (int q = 0; q < 5; ++q) w[SweepSrc<DIR, S>::perm(q)] = WL[q];
-            visc_over_p(f, w, tau_n, tau_d);
-        }
+        // collision time mu / p at the left cell (update.cpp:262-264), stored by
+        // this step's x-sweep reconstruction
+        const double tau_n = __ldg(f.tau[0] + x.c), tau_d = __ldg(f.tau[1] + x.c);
         FluxConst fc;
         fc.gm1 = f.gm1;
         fc.hig = 0.5 * (f.icT * f.iR); // R / (gamma - 1) * 1 / R

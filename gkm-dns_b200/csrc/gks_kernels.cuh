@@ -18,6 +18,7 @@ struct FieldDev {
     double *W[5];     // state, interior layout
     double *rec[10];  // Wl[0..4], Wr[0..4] of the current sweep
     double *F[15];    // Fx[0..4], Fy[0..4], Fz[0..4]
+    double *tau[2];   // mu/p of each cell as numerator / denominator, set by the x-sweep reconstruction
     const double *spl_cp;   // natural-spline Thomas coefficients, nt entries
     const double *spl_inv;  // reciprocal pivots, nt entries
     long long base;   // first work item of this field in the batch (a multiple of kItemAlign)
