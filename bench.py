@@ -504,7 +504,7 @@ def run_ours(args):
             "config": {"workload": f"DHIT {nc}^3 WENO-GKS step, FP64 parity path", "nc": nc, "k0": K0,
                        "mach_t": args.mach, "re_lambda": args.re, "cfl": CFL, "precision": "fp64",
                        "parallelism": f"replicas x{ws}",
-                       "l2": f"working set {30 * 8 * nc ** 3 / 1e6:.0f} MB per field (state {40 * nc ** 3 / 1e6:.0f} MB)"
+                       "l2": f"working set {32 * 8 * nc ** 3 / 1e6:.0f} MB per field (state {40 * nc ** 3 / 1e6:.0f} MB)"
                              " vs 126 MB L2, no flush"},
             "mixed": {"value": mixed_value, "ms_per_step": results["mixed"]["ms"],
                       "speedup_vs_fp64": mixed_value / value,
