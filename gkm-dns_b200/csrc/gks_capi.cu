@@ -266,7 +266,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         const gks_phys &p = phys[f];
         const long long n = (long long)p.nc * p.nc * p.nc;
         if (cudaMalloc(&h.mem, (size_t)32 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
-        cudaMemset(h.mem, 0, (size_t)32 * n * sizeof(double));
+        if (cudaMemset(h.mem, 0, (size_t)32 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ECUDA);
         FieldDev &d = h.dev;
         memset(&d, 0, sizeof(d));
         for (int q = 0; q < 5; ++q) d.W[q] = h.mem + q * n;
@@ -277,8 +277,9 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         std::vector<double> cp, inv;
         spline_coeffs(nt, cp, inv);
         if (cudaMalloc(&h.spl, 2 * (size_t)nt * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
-        cudaMemcpy(h.spl, cp.data(), nt * sizeof(double), cudaMemcpyHostToDevice);
-        cudaMemcpy(h.spl + nt, inv.data(), nt * sizeof(double), cudaMemcpyHostToDevice);
+        if (cudaMemcpy(h.spl, cp.data(), nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h.spl + nt, inv.data(), nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(GKS_ECUDA);
         d.spl_cp = h.spl;
         d.spl_inv = h.spl + nt;
         d.base = base;
@@ -325,12 +326,13 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     }
     if (cudaMalloc(&ctx->d_fields, nfields * sizeof(FieldDev)) != cudaSuccess) return bail(GKS_ENOMEM);
     for (int f = 0; f < nfields; ++f)
-        cudaMemcpy(ctx->d_fields + f, &ctx->fh[f].dev, sizeof(FieldDev), cudaMemcpyHostToDevice);
+        if (cudaMemcpy(ctx->d_fields + f, &ctx->fh[f].dev, sizeof(FieldDev), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(GKS_ECUDA);
     if (cudaMalloc(&ctx->d_partial, (size_t)148 * 32 * 24 * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
     if (cudaMalloc(&ctx->d_sums, 32 * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
     if (cudaMalloc(&ctx->d_bits, sizeof(unsigned long long)) != cudaSuccess) return bail(GKS_ENOMEM);
     if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return bail(GKS_ENOMEM);
-    cudaMemset(ctx->d_err, 0, sizeof(int));
+    if (cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess) return bail(GKS_ECUDA);
     ctx->batch.fields = ctx->d_fields;
     ctx->batch.nfields = nfields;
     ctx->batch.total = base;
