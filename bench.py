@@ -17,10 +17,13 @@ ours       K timed steps of the FP64 path (the parity path, `value`) and of the
            sweep) timed live with CUDA events against the FP64 FMA peak
            measured live on the same GPU.  Under torchrun every rank advances
            its own replica (replicas only: the path does not shard).
+           The line also carries the mixed path's accuracy against the FP64
+           path on the same field run to t/t0 = 2 (statistics every 10 steps).
 reference  the reference's own CPU implementation (oracle/_ref, compiled from
-           its sources) on the host cores: one process per core (at most 64),
-           each timing the reference step on a 2-plane y-slab of the same
-           256^3 field (about 1 s of CPU per step and process).
+           its sources) on the host cores: the 256^3 field cut into P y-slabs
+           (P the largest power of two up to the core count, at most 64), one
+           process per slab, so that every timed step advances the whole
+           field; ms_per_step is the slowest process's measured time per step.
 """
 
 from __future__ import annotations
@@ -51,6 +54,9 @@ OPS_FLUX = 8005 + 90 + 25
 OPS_RECON = 1122
 OPS_CELL = 3 * (OPS_FLUX + OPS_RECON) + 30
 BYTES_CELL = 80  # 5 doubles read + 5 written per cell-update
+# FP64 FMA lanes per SM of B200 (sm_100): the nominal FP64 rate is
+# SMs x 64 x 2 flops x SM clock
+FP64_LANES_PER_SM = 64
 
 
 def dist_env():
@@ -188,6 +194,14 @@ def read_traffic(nc: int):
     return None if b is None else b * nc ** 3
 
 
+def bench_config(nc: int, mach: float, re: float, ws: int) -> dict:
+    """The workload both arms time (identical keys and values in both lines)."""
+    return {"workload": f"DHIT {nc}^3 WENO-GKS step, FP64 parity path", "nc": nc, "k0": K0, "mach_t": mach,
+            "re_lambda": re, "cfl": CFL, "precision": "fp64", "parallelism": f"replicas x{ws}",
+            "l2": f"working set {32 * 8 * nc ** 3 / 1e6:.0f} MB per field (state {40 * nc ** 3 / 1e6:.0f} MB)"
+                  " vs 126 MB L2, no flush"}
+
+
 def make_case(nc: int, seed: int, mach: float = MACH, re: float = RE):
     import gks_ic
 
@@ -298,75 +312,163 @@ def run_ensemble(gks, gks_ic, torch, steps: int, warmup: int, local: int, tune: 
     return out
 
 
-def run_accuracy(args):
-    """Mixed vs FP64 on the same field to t/t0 = args.t_end (statistics every 10
-    steps): relative errors of the statistics, and each precision's step time
-    (CUDA events over 10 further steps)."""
+def accuracy_history(gks, torch, nc: int, mach: float, re: float, t_end: float, control: bool = False,
+                     stats_every: int = 10) -> dict:
+    """Mixed vs FP64 on the same field to t/t0 = t_end (statistics every
+    `stats_every` steps): relative errors of the statistics at the end and their
+    largest value over the history.  With control, the second run is the FP64
+    path started from the initial field rounded to FP32 (no FP32 arithmetic),
+    the size of difference any FP32-rounding perturbation grows into."""
     import numpy as np
-    import torch
 
-    import gks_b200 as gks
     import gks_ic
 
-    nc = args.nc
-    case = make_case(nc, 0, args.mach, args.re)
+    case = make_case(nc, 0, mach, re)
     W = gks_ic.to_conservative_padded(case)
-    hist, ms = {}, {}
-    # the control: a perturbation of FP32-rounding size in the initial field only
-    W32 = W.astype(np.float32).astype(np.float64) if args.control else None
-    runs = (("fp64", gks.FP64, W), ("mixed", gks.FP64 if args.control else gks.MIXED, W32 if args.control else W))
+    hist = {}
+    W32 = W.astype(np.float32).astype(np.float64) if control else None
+    runs = (("fp64", gks.FP64, W), ("mixed", gks.FP64 if control else gks.MIXED, W32 if control else W))
+    nsteps = dt = None
     for name, prec, w0 in runs:
         with gks.Solver(gks.phys_from_case(case), prec) as s:
             s.upload(w0)
             dt = s.timestep(CFL)
-            nsteps = int(np.ceil(args.t_end * case.t0 / dt))
+            nsteps = int(np.ceil(t_end * case.t0 / dt))
             h = []
             for k in range(nsteps + 1):
-                if k % 10 == 0 or k == nsteps:
+                if k % stats_every == 0 or k == nsteps:
                     h.append(s.stats())
                 if k < nsteps:
                     s.step(1)
             s.sync()
             hist[name] = h
-            ms[name] = timed_steps(s, 10, torch)
     keys = ("tke", "diss", "skew_u", "skew_v", "skew_w")
     final = {k: abs(hist["mixed"][-1][k] - hist["fp64"][-1][k]) / abs(hist["fp64"][-1][k]) for k in keys}
     worst = {k: max(abs(a[k] - b[k]) / abs(b[k]) for a, b in zip(hist["mixed"], hist["fp64"])) for k in keys}
-    print(json.dumps({"mode": "accuracy-control" if args.control else "accuracy", "nc": nc, "mach_t": args.mach, "re_lambda": args.re,
-                      "t_over_t0": args.t_end, "steps": nsteps, "dt": dt,
-                      "rel_err_final": final, "rel_err_max_over_history": worst,
-                      "tke_fp64_initial": hist["fp64"][0]["tke"], "tke_fp64_final": hist["fp64"][-1]["tke"],
-                      "diss_fp64_final": hist["fp64"][-1]["diss"],
-                      "ms_per_step": ms, "cell_updates_per_s": {k: nc ** 3 / (v * 1e-3) for k, v in ms.items()},
-                      "mixed_speedup": ms["fp64"] / ms["mixed"]}))
+    return {"nc": nc, "mach_t": mach, "re_lambda": re, "t_over_t0": t_end, "steps": nsteps, "dt": dt,
+            "stats_every": stats_every, "rel_err_final": final, "rel_err_max_over_history": worst,
+            "tke_fp64_initial": hist["fp64"][0]["tke"], "tke_fp64_final": hist["fp64"][-1]["tke"],
+            "diss_fp64_final": hist["fp64"][-1]["diss"]}
+
+
+def run_accuracy(args):
+    """Mixed vs FP64 on the same field to t/t0 = args.t_end, plus each
+    precision's step time (CUDA events over 10 further steps)."""
+    import torch
+
+    import gks_b200 as gks
+
+    acc = accuracy_history(gks, torch, args.nc, args.mach, args.re, args.t_end, args.control)
+    case = make_case(args.nc, 0, args.mach, args.re)
+    import gks_ic
+
+    ms = {}
+    for name, prec in (("fp64", gks.FP64), ("mixed", gks.MIXED)):
+        with gks.Solver(gks.phys_from_case(case), prec) as s:
+            s.upload(gks_ic.to_conservative_padded(case))
+            s.timestep(CFL)
+            s.step(3)
+            s.sync()
+            ms[name] = timed_steps(s, 10, torch)
+    acc.update({"mode": "accuracy-control" if args.control else "accuracy", "ms_per_step": ms,
+                "cell_updates_per_s": {k: args.nc ** 3 / (v * 1e-3) for k, v in ms.items()},
+                "mixed_speedup": ms["fp64"] / ms["mixed"]})
+    print(json.dumps(acc))
     return 0
 
 
+def reference_slabs(nc: int, cores: int) -> int:
+    """Processes of the reference arm: the largest power of two up to `cores`
+    (at most 64) that divides nc, one y-slab each."""
+    p = 1
+    while p * 2 <= min(cores, 64) and nc % (p * 2) == 0:
+        p *= 2
+    return p
+
+
 def run_reference(args):
+    """The reference's own CPU step on the whole field: P processes, each
+    advancing its own y-slab (Init<a>00, as rank a of a P x 1 x 1 grid reads
+    it), all started together; a step is every slab's evolveEulerian +
+    HaloTransfer, timed by each process, and the job's step time is the slowest
+    process's."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    procs = max(1, min(len(os.sched_getaffinity(0)), 64))
-    warm, steps = max(0, args.warmup), max(1, args.steps)
-    cb = cpu_baseline(NC, steps, warm, planes=2, procs=procs)
-    if cb is None:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gks_ic
+    import pyoracle
+
+    if not os.path.exists(pyoracle.REF_HARNESS_FAST):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness_fast is not built"}))
         return 0
+    nc = args.nc
+    cores = len(os.sched_getaffinity(0))
+    P = reference_slabs(nc, cores)
+    planes = nc // P
+    warm, steps = max(0, args.warmup), max(1, args.steps)
+    d = tempfile.mkdtemp(prefix="gks_refarm_")
+    gks_ic.write_case(d, make_case(nc, 0, args.mach, args.re), slab_planes=planes, all_slabs=True)
+    ps = [subprocess.Popen(pyoracle.ref_time_cmd(d, steps, P, CFL, warm) + [str(a)], stdout=subprocess.PIPE,
+                           text=True) for a in range(P)]
+    res = []
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference step process exited {p.returncode}"}))
+            return 0
+        res.append(json.loads(out.strip().splitlines()[-1]))
+    secs = max(r["seconds"] for r in res)
+    cells = sum(r["cells"] for r in res)
+    assert cells == nc ** 3 and sorted(r["slab_index"] for r in res) == list(range(P))
+    value = cells * steps / secs
+    sample = (f"the whole {nc}^3 field every step: {P} reference processes (update.cpp evolveEulerian + "
+              f"HaloTransfer, g++ -O3 -march=x86-64-v3), each on its own {planes}x{nc}x{nc} y-slab; "
+              f"{steps} timed steps after {warm} warm-up; slowest process")
     line = {
-        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": 0,
-        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * NC ** 3 / cb["value"], "higher_is_better": True,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"DHIT {NC}^3 WENO-GKS step (FP64), reference CPU path",
-                   "nc": NC, "k0": K0, "mach_t": MACH, "re_lambda": RE, "cfl": CFL},
-        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": bench_config(nc, args.mach, args.re, ws),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "per_process_ms_per_step": sorted(1e3 * r["seconds"] / steps for r in res),
     }
     print(json.dumps(line))
     return 0
 
 
+def measure_peaks(gks, uuid: str) -> dict:
+    """FP64 / FP32 FMA peaks measured here (no FP64 figure is supplied): a first
+    short burst, then the FP64 probe repeated for about 1.5 s with the SM clock
+    sampled, whose settled rate (median of the second half) is the sustained
+    peak that a kernel timed inside the long step loop is compared with; the
+    nominal rate (SMs x 64 FP64 FMA lanes x 2 flops x clock) is given at the
+    probe's clock and at the maximum clock, to locate the probe's gap."""
+    import torch
+
+    burst = gks.peak_tflops(gks.FP64)
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    runs, t0 = [], time.perf_counter()
+    while time.perf_counter() - t0 < 1.5:
+        runs.append(gks.peak_tflops(gks.FP64))
+    clk = sampler.stop()
+    peak64 = statistics.median(runs[len(runs) // 2:])
+    peak32 = gks.peak_tflops(gks.MIXED)
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    out = {"fp64": peak64, "fp64_burst": burst, "fp32": peak32, "sms": nsm, "probe_clocks": clk}
+    if clk:
+        at_probe = nsm * FP64_LANES_PER_SM * 2 * clk["sm_mhz"] * 1e6 / 1e12
+        at_max = nsm * FP64_LANES_PER_SM * 2 * clk["sm_max_mhz"] * 1e6 / 1e12
+        out["fp64_nominal_at_probe_clock"] = at_probe
+        out["fp64_nominal_at_max_clock"] = at_max
+        out["probe_frac_of_nominal_at_probe_clock"] = peak64 / at_probe
+        out["probe_frac_of_nominal_at_max_clock"] = peak64 / at_max
+    return out
+
+
 def run_ours(args):
-    import numpy as np
     import torch
 
     import gks_b200 as gks
@@ -382,16 +484,8 @@ def run_ours(args):
     phys = gks.phys_from_case(case)
     uuid = gpu_uuid(local)
 
-    # peaks of the FP64 / FP32 pipes, measured here (no FP64 figure is supplied):
-    # a first short burst, then the probe repeated for about 1.5 s, whose
-    # settled rate (median of the second half) is the sustained peak that a
-    # kernel timed inside the long step loop is compared with
-    peak64_burst = gks.peak_tflops(gks.FP64)
-    runs, t0 = [], time.perf_counter()
-    while time.perf_counter() - t0 < 1.5:
-        runs.append(gks.peak_tflops(gks.FP64))
-    peak64 = statistics.median(runs[len(runs) // 2:])
-    peak32 = gks.peak_tflops(gks.MIXED)
+    peaks = measure_peaks(gks, uuid)
+    peak64 = peaks["fp64"]
     hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -468,23 +562,30 @@ def run_ours(args):
     s.close()
     bytes_io = 5 * nt ** 3 * 8
 
+    # the mixed path's accuracy against FP64 to t/t0 = 2 on the same field
+    acc = None
+    if not args.no_accuracy:
+        acc = accuracy_history(gks, torch, nc, args.mach, args.re, 2.0)
+
     cells = nc ** 3
     value = whole_job_rate(ws, cells, results["fp64"]["ms"])
     mixed_value = whole_job_rate(ws, cells, results["mixed"]["ms"])
     flux_ms = statistics.mean(stages["fp64"][k] for k in ("flux_x", "flux_y", "flux_z"))
     recon_ms = statistics.mean(stages["fp64"][k] for k in ("recon_x", "recon_y", "recon_z"))
-    achieved = OPS_FLUX * cells / (flux_ms * 1e-3) / 1e12
+    flux_s = flux_ms * 1e-3
     traffic = read_traffic(nc)
-    # hardware view: FP64 instructions the flux kernel executes per interface
-    # (ncu, committed summary) against the FP64 FMA instruction rate (peak / 2)
+    # this algorithm's FP64 arithmetic per interface (ncu op counts of the flux
+    # kernel, committed summary: 2 flops per DFMA, 1 per DMUL / DADD)
+    flops = read_profile("flux_fp64_ncu.txt", "fp64_flops_per_interface")
     inst = read_profile("flux_fp64_ncu.txt", "fp64_inst_per_interface")
+    achieved = flops * cells / flux_s / 1e12 if flops else None
     fp64_pipe = None
     if inst:
-        rate = inst * cells / (flux_ms * 1e-3) / 1e12
+        rate = inst * cells / flux_s / 1e12
         fp64_pipe = {"inst_per_interface": inst, "achieved_tinst_s": rate, "peak_tinst_s": peak64 / 2,
                      "frac": rate / (peak64 / 2),
-                     "note": "the reference's operation count (ops_per_interface) exceeds the FP64 "
-                             "instructions this algorithm executes; frac here is FP64-pipe utilisation"}
+                     "note": "FP64 instructions per second against the FP64 FMA instruction rate: "
+                             "pipe utilisation (a DMUL or DADD occupies the pipe like a DFMA)"}
     st64, st32 = results["fp64"]["stats"], results["mixed"]["stats"]
     rel = {k: abs(st32[k] - st64[k]) / abs(st64[k]) for k in ("tke", "diss", "skew_u", "skew_v", "skew_w")}
 
@@ -501,25 +602,28 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": f"synthetic: seeded solenoidal DHIT field (k0 4, Mt {args.mach:g}, Re_lambda {args.re:g}), "
                     "one replica per GPU",
-            "config": {"workload": f"DHIT {nc}^3 WENO-GKS step, FP64 parity path", "nc": nc, "k0": K0,
-                       "mach_t": args.mach, "re_lambda": args.re, "cfl": CFL, "precision": "fp64",
-                       "parallelism": f"replicas x{ws}",
-                       "l2": f"working set {32 * 8 * nc ** 3 / 1e6:.0f} MB per field (state {40 * nc ** 3 / 1e6:.0f} MB)"
-                             " vs 126 MB L2, no flush"},
-            "mixed": {"value": mixed_value, "ms_per_step": results["mixed"]["ms"],
-                      "speedup_vs_fp64": mixed_value / value,
-                      "rel_err_vs_fp64_after_steps": rel, "steps_compared": args.warmup + args.steps,
-                      "dtype": "f32 weno/slopes/slope moments + f64 moments/erfc/update/reductions",
-                      "stage_ms": stages["mixed"]},
+            "config": bench_config(nc, args.mach, args.re, ws),
             "roofline": {"bound": "fp64", "kernel": "flux sweep (k_flux, FP64)", "achieved": achieved,
-                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": traffic,
+                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64 if achieved else None,
+                         "traffic": traffic,
+                         "flops_per_interface": flops,
+                         "flops_source": "FP64 flops the co-moving-frame flux executes per interface "
+                                         "(2 x DFMA + DMUL + DADD, profiles/flux_fp64_ncu.txt)",
                          "peak_source": "FP64 FMA peak measured live by gks_peak_flops on this GPU, sustained"
                                         " (the probe repeated for 1.5 s; the kernel is timed inside the step loop)",
-                         "peak_burst": peak64_burst,
-                         "ops_per_interface": OPS_FLUX, "launch_ms": flux_ms,
+                         "peak_burst": peaks["fp64_burst"], "launch_ms": flux_ms,
                          "fp64_pipe": fp64_pipe,
-                         "step_achieved": OPS_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e12,
-                         "fp32_peak": peak32},
+                         "probe": {k: peaks.get(k) for k in ("sms", "probe_clocks", "fp64_nominal_at_probe_clock",
+                                                             "fp64_nominal_at_max_clock",
+                                                             "probe_frac_of_nominal_at_probe_clock",
+                                                             "probe_frac_of_nominal_at_max_clock")},
+                         "reference_ops_equivalent": {
+                             "ops_per_interface": OPS_FLUX,
+                             "tflops": OPS_FLUX * cells / flux_s / 1e12,
+                             "step_tflops": OPS_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e12,
+                             "note": "the reference formulation's operation count (MCal contractions); "
+                                     "not a roofline fraction"},
+                         "fp32_peak": peaks["fp32"]},
             "hbm": {"achieved_gbs": BYTES_CELL * cells / (results["fp64"]["ms"] * 1e-3) / 1e9,
                     "peak_gbs": hbm_peak, "peak_source": hbm_src,
                     "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
@@ -537,6 +641,21 @@ def run_ours(args):
             line["cpu_baseline"] = cb
         if rg:
             line["reference_gpu"] = rg
+        line["mixed"] = {"value": mixed_value, "ms_per_step": results["mixed"]["ms"],
+                         "speedup_vs_fp64": mixed_value / value,
+                         "rel_err_vs_fp64_after_steps": rel, "steps_compared": args.warmup + args.steps,
+                         "dtype": "f32 weno/slopes/slope moments + f64 moments/erfc/update/reductions",
+                         "stage_ms": stages["mixed"], "accuracy_t2": acc}
+        # compact summary last, so that the end of the line carries it
+        line["headline"] = {
+            "fp64_cell_updates_per_s": value, "mixed_cell_updates_per_s": mixed_value,
+            "mixed_over_fp64": mixed_value / value,
+            "e2e_cell_updates_per_s": line["e2e"]["value"],
+            "flux_fp64_pipe_frac": fp64_pipe["frac"] if fp64_pipe else None,
+            "mixed_rel_err_t2_final": {k: acc["rel_err_final"][k] for k in ("tke", "diss")} if acc else None,
+            "mixed_rel_err_t2_max": {k: acc["rel_err_max_over_history"][k] for k in ("tke", "diss")} if acc else None,
+            "stats_ms": stats_ms,
+        }
         print(json.dumps(line))
     dist.close()
     return 0
@@ -553,6 +672,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="keep the untuned launch configuration")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 96-field ensemble line")
     ap.add_argument("--no-refgpu", action="store_true", help="skip timing the reference's own GPU path")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the mixed-vs-FP64 run to t/t0 = 2")
     ap.add_argument("--accuracy", action="store_true", help="mixed vs FP64 statistics to t/t0 = --t-end, then exit")
     ap.add_argument("--t-end", type=float, default=2.0, help="accuracy run length in eddy turnover times")
     ap.add_argument("--control", action="store_true",

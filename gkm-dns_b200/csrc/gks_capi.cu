@@ -41,7 +41,7 @@ struct gks_ctx {
     int precision = 0;
     int flags = 0;
     int device = 0;
-    int nsm = 148;
+    int nsm = 0; // SMs of the device, set by gks_create
     std::vector<FieldHost> fh;
     FieldDev *d_fields = nullptr;
     gks::Batch batch{};
@@ -328,7 +328,8 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     for (int f = 0; f < nfields; ++f)
         if (cudaMemcpy(ctx->d_fields + f, &ctx->fh[f].dev, sizeof(FieldDev), cudaMemcpyHostToDevice) != cudaSuccess)
             return bail(GKS_ECUDA);
-    if (cudaMalloc(&ctx->d_partial, (size_t)148 * 32 * 24 * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+    if (cudaMalloc(&ctx->d_partial, gks::stats_partial_elems(ctx->nsm) * sizeof(double)) != cudaSuccess)
+        return bail(GKS_ENOMEM);
     if (cudaMalloc(&ctx->d_sums, 32 * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
     if (cudaMalloc(&ctx->d_bits, sizeof(unsigned long long)) != cudaSuccess) return bail(GKS_ENOMEM);
     if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return bail(GKS_ENOMEM);
@@ -377,7 +378,7 @@ int gks_upload(gks_ctx *ctx, int f, double *const W[5])
     const size_t nt = (size_t)ctx->fh[f].phys.nc + 6, Nt = nt * nt * nt;
     for (int q = 0; q < 5; ++q)
         CK(cudaMemcpyAsync(ctx->d_stage + q * Nt, W[q], Nt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(gks::launch_gather(ctx->fh[f].dev, ctx->d_stage, ctx->stream));
+    CK(gks::launch_gather(ctx->fh[f].dev, ctx->d_stage, ctx->nsm, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->fh[f].uploaded = true;
     return GKS_OK;
@@ -393,7 +394,7 @@ int gks_download(gks_ctx *ctx, int f, double *const W[5])
     CK(cudaSetDevice(ctx->device));
     if ((rc = ensure_stage(ctx, f))) return rc;
     const size_t nt = (size_t)ctx->fh[f].phys.nc + 6, Nt = nt * nt * nt;
-    CK(gks::launch_scatter(ctx->fh[f].dev, ctx->d_stage, ctx->stream));
+    CK(gks::launch_scatter(ctx->fh[f].dev, ctx->d_stage, ctx->nsm, ctx->stream));
     for (int q = 0; q < 5; ++q)
         CK(cudaMemcpyAsync(W[q], ctx->d_stage + q * Nt, Nt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -419,7 +420,7 @@ int gks_timestep(gks_ctx *ctx, int f, double cfl, double *dt_out)
     if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "timestep before upload");
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemsetAsync(ctx->d_bits, 0, sizeof(unsigned long long), ctx->stream));
-    CK(gks::launch_maxwave(ctx->fh[f].dev, ctx->d_bits, ctx->stream));
+    CK(gks::launch_maxwave(ctx->fh[f].dev, ctx->d_bits, ctx->nsm, ctx->stream));
     unsigned long long bits = 0;
     CK(cudaMemcpyAsync(&bits, ctx->d_bits, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -466,7 +467,7 @@ int gks_check(gks_ctx *ctx)
     CK(cudaSetDevice(ctx->device));
     for (int f = 0; f < ctx->nfields; ++f) {
         CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
-        CK(gks::launch_check(ctx->fh[f].dev, ctx->d_err, ctx->stream));
+        CK(gks::launch_check(ctx->fh[f].dev, ctx->d_err, ctx->nsm, ctx->stream));
         int word = 0;
         int rc = read_err(ctx, &word, true);
         if (rc) return rc;
@@ -483,7 +484,7 @@ int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
     if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "stats before upload");
     CK(cudaSetDevice(ctx->device));
     const FieldDev &d = ctx->fh[f].dev;
-    CK(gks::launch_stats(d, d.F[0], ctx->d_partial, ctx->d_sums, ctx->stream));
+    CK(gks::launch_stats(d, d.F[0], ctx->d_partial, ctx->d_sums, ctx->nsm, ctx->stream));
     double s[24];
     CK(cudaMemcpyAsync(s, ctx->d_sums, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

@@ -924,7 +924,7 @@ __global__ void __launch_bounds__(32 * kSplTiledWarps) k_spline_tiled(FieldDev f
     }
 }
 
-constexpr int NSUM1 = 24;
+constexpr int NSUM1 = kStatsSums;
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -1040,14 +1040,6 @@ __global__ void k_check(FieldDev f, int *err)
     }
 }
 
-int grid_for(long long items, int block)
-{
-    long long g = (items + block - 1) / block;
-    if (g > 148LL * 32) g = 148LL * 32;
-    if (g < 1) g = 1;
-    return int(g);
-}
-
 template <typename KernelT>
 cudaError_t occ(KernelT k, int block, int *n)
 {
@@ -1158,29 +1150,29 @@ cudaError_t max_resident_blocks(int kind, int dir, int prec, int variant, int bl
     return prec == 0 ? occ_dir<0>(kind, dir, variant, block, n) : occ_dir<1>(kind, dir, variant, block, n);
 }
 
-cudaError_t launch_gather(const FieldDev &f, const double *stage, cudaStream_t st)
+cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaStream_t st)
 {
-    k_gather<<<grid_for(f.ncell, 256), 256, 0, st>>>(f, stage);
+    k_gather<<<helper_grid(f.ncell, 256, nsm), 256, 0, st>>>(f, stage);
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter(const FieldDev &f, double *stage, cudaStream_t st)
+cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st)
 {
     const long long nt = f.nc + 6;
-    k_scatter<<<grid_for(nt * nt * nt, 256), 256, 0, st>>>(f, stage);
+    k_scatter<<<helper_grid(nt * nt * nt, 256, nsm), 256, 0, st>>>(f, stage);
     return cudaGetLastError();
 }
 
-cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, cudaStream_t st)
+cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int nsm, cudaStream_t st)
 {
-    k_maxwave<<<grid_for(f.ncell, 256), 256, 0, st>>>(f, out_bits);
+    k_maxwave<<<helper_grid(f.ncell, 256, nsm), 256, 0, st>>>(f, out_bits);
     return cudaGetLastError();
 }
 
-cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, cudaStream_t st)
+cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st)
 {
     const int block = 256;
-    const int grid = std::min(grid_for(f.ncell, block), 148 * 8);
+    const int grid = stats_grid(f.ncell, block, nsm); // partial holds stats_partial_elems(nsm) >= kStatsSums * grid
     k_velocity<<<grid, block, 0, st>>>(f, scratch);
     const long long lines = (long long)f.nc * f.nc;
     auto lgrid = [&](int nw) { return int((lines + kSplLines * nw - 1) / (kSplLines * nw)); };
@@ -1192,9 +1184,9 @@ cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, do
     return cudaGetLastError();
 }
 
-cudaError_t launch_check(const FieldDev &f, int *err, cudaStream_t st)
+cudaError_t launch_check(const FieldDev &f, int *err, int nsm, cudaStream_t st)
 {
-    k_check<<<grid_for(f.ncell, 256), 256, 0, st>>>(f, err);
+    k_check<<<helper_grid(f.ncell, 256, nsm), 256, 0, st>>>(f, err);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "gks_limits.h"
+
 namespace gks {
 
 struct FieldDev {
@@ -89,19 +91,19 @@ cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st);
 cudaError_t max_resident_blocks(int kind, int dir, int prec, int variant, int block, int *blocks_per_sm);
 
 // Layout conversion of one field: padded host layout (5 x nt^3, contiguous) <-> interior.
-cudaError_t launch_gather(const FieldDev &f, const double *stage, cudaStream_t st);
-cudaError_t launch_scatter(const FieldDev &f, double *stage, cudaStream_t st);
+cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaStream_t st);
+cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st);
 
 // max(|u| + c) over the interior of one field into *out_bits (uint64 image of a positive double;
 // *out_bits must be zero on entry).
-cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, cudaStream_t st);
+cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int nsm, cudaStream_t st);
 
-// Statistics of one field.  scratch: 12 * nc^3 doubles; partial: >= 24 * nblocks doubles.
+// Statistics of one field.  scratch: 12 * nc^3 doubles; partial: stats_partial_elems(nsm) doubles.
 // Writes 24 means into sums[0..23]: the 18 PrintStats means and, for p, T and
 // 1/rho, the means of x - K and (x - K)^2 (K = the value at cell 0).
-cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, cudaStream_t st);
+cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st);
 
 // Scan a field for non-finite values or non-positive density / pressure; sets bit 1 of *err.
-cudaError_t launch_check(const FieldDev &f, int *err, cudaStream_t st);
+cudaError_t launch_check(const FieldDev &f, int *err, int nsm, cudaStream_t st);
 
 } // namespace gks

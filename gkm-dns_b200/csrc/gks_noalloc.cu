@@ -13,18 +13,28 @@
 //   [0, kBlocks)      per-block maxima (bit images of non-negative doubles)
 //   [kBlocks]         arrival counter of the blocks of one call
 //   [kBlocks + 1]     the field's maximum, written by the last block
-// Every call writes all kBlocks partial slots and clears the counter and
-// the result before its kernel runs, so nothing of the previous call leaks
-// in.  Calls share the array: two calls whose kernels overlap on the GPU
-// (different streams, or threads) race on it and must be serialised by the
-// caller.
+// A call launches `grid` <= kBlocks blocks; block b writes slot b, and the
+// last block to arrive reads slots [0, grid) only, so slots left over from an
+// earlier call with a larger grid are never read.  The counter and the result
+// are cleared before every launch.  Calls share the array: two calls whose
+// kernels overlap on the GPU (different streams, or threads) race on it and
+// must be serialised by the caller.
+//
+// The array's device address is looked up (cudaGetSymbolAddress) once per
+// device and CUDA context, with that device current, on the first call there:
+// a host-side mention of g_noalloc_scratch names a host stand-in, not device
+// memory.  If the context is replaced (cudaDeviceReset, then new work), the
+// next call sees a new context id and looks the address up again.
 #include "../../include/gks_b200.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
 #include <mutex>
+
+#include "gks_limits.h"
 
 namespace {
 
@@ -93,20 +103,42 @@ __global__ void __launch_bounds__(kThreads) k_maxwave_noalloc(Fields f, long lon
 }
 
 std::mutex g_setup_mu;
-unsigned long long *g_scratch_addr[kMaxDevices] = {};
+gks::ContextAddressCache<kMaxDevices> g_scratch_cache;
 
-// Device address of the scratch on `dev` (looked up once per device, with
-// that device current).
+// Unique id of the calling thread's current CUDA context (cuCtxGetId, reached
+// through the runtime's driver entry point so the library needs no link to the
+// driver library); 0 where the driver does not provide it.
+unsigned long long current_context_id()
+{
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetId fn = []() -> GetId {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return (GetId)p;
+    }();
+    unsigned long long id = 0;
+    if (fn && fn(nullptr, &id) != CUDA_SUCCESS) id = 0;
+    return id;
+}
+
+// Device address of the scratch on `dev` in its current context.
 int scratch_for(int dev, unsigned long long **out)
 {
     if (dev < 0 || dev >= kMaxDevices) return GKS_EINVAL;
+    // make the device's primary context current (it exists from here on), so
+    // that its id and the symbol lookup below refer to the same context
+    if (cudaSetDevice(dev) != cudaSuccess) return GKS_ECUDA;
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GKS_ECUDA;
-        g_scratch_addr[dev] = (unsigned long long *)p;
-    }
-    *out = g_scratch_addr[dev];
+    void *p = nullptr;
+    const int rc = g_scratch_cache.get(dev, ctx, [](void **a) {
+        return cudaGetSymbolAddress(a, g_noalloc_scratch) == cudaSuccess ? 0 : 1;
+    }, &p);
+    if (rc != 0) return GKS_ECUDA;
+    *out = (unsigned long long *)p;
     return GKS_OK;
 }
 

@@ -164,19 +164,25 @@ def file_order(a: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()
 
 
-def write_case(casedir: str, case: DhitCase, slab_planes: int | None = None) -> None:
-    """Write params, particleCount and Init000.  With slab_planes, Init000 holds
-    only the first slab_planes y-planes: the block of process (0,0,0) on a
-    (nc/slab_planes) x 1 x 1 process grid."""
+def write_case(casedir: str, case: DhitCase, slab_planes: int | None = None, all_slabs: bool = False) -> None:
+    """Write params, particleCount and Init000.  With slab_planes, the y-slabs
+    of slab_planes planes are the blocks of an (nc/slab_planes) x 1 x 1 process
+    grid: Init000 holds the first slab_planes y-planes (process (0,0,0)) and,
+    with all_slabs, Init<a>00 holds slab a for every process a, the file each
+    rank's Initialize_DHIT reads (FlowField.cpp:73-75)."""
     ic = os.path.join(casedir, "InitialConditions")
     os.makedirs(ic, exist_ok=True)
     write_params(os.path.join(ic, "params"), case)
     with open(os.path.join(ic, "particleCount"), "wb") as f:
         f.write(struct.pack("<i", 0))
-    sl = slice(0, slab_planes) if slab_planes else slice(None)
-    with open(os.path.join(ic, "Init000"), "wb") as f:
-        for a in (case.u, case.v, case.w, case.rho, case.p):
-            f.write(file_order(np.ascontiguousarray(a[sl])).astype("<f8").tobytes())
+    if slab_planes and case.nc % slab_planes:
+        raise ValueError(f"{slab_planes} planes do not divide nc = {case.nc}")
+    nslab = case.nc // slab_planes if (slab_planes and all_slabs) else 1
+    for a in range(nslab):
+        sl = slice(a * slab_planes, (a + 1) * slab_planes) if slab_planes else slice(None)
+        with open(os.path.join(ic, f"Init{a}00"), "wb") as f:
+            for arr in (case.u, case.v, case.w, case.rho, case.p):
+                f.write(file_order(np.ascontiguousarray(arr[sl])).astype("<f8").tobytes())
 
 
 def read_init(casedir: str) -> tuple[dict, np.ndarray]:

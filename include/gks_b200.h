@@ -177,12 +177,14 @@ int gks_peak_flops(int precision, double *tflops);
  * dW: the caller's five device arrays in this library's interior layout
  * (nc^3 doubles each, index (j*nc + i)*nc + k), e.g. from gks_device_fields.
  * Returns dt = cfl * (2 pi/nc) / max(|u| + c) in *dt_out (host memory), the
- * same value gks_timestep gives, after synchronising `stream` (NULL: the
- * legacy default stream).  Limit: nc <= 1024, else GKS_ETOOBIG.  Scratch is a
- * fixed file-scope device array of 1026 64-bit words that every GPU loading
- * the library holds until exit; the first call on a device looks up its
- * address, so make that first call before any stream capture.  Calls share
- * the scratch: calls that overlap on the GPU race and must be serialised. */
+ * same value gks_timestep gives; it synchronises `stream` (NULL: the legacy
+ * default stream) to hand dt back.  Limit: nc <= 1024, else GKS_ETOOBIG.
+ * Scratch is a fixed file-scope device array of 1026 64-bit words that every
+ * GPU loading the library holds until exit; the first call on a device (and
+ * the first after its CUDA context is replaced, e.g. by cudaDeviceReset)
+ * looks up the array's address, so make that first call before any stream
+ * capture.  Calls share the scratch: calls that overlap on the GPU race and
+ * must be serialised. */
 int gks_timestep_noalloc(const double *const dW[5], int nc, double gam, double cfl, void *stream,
                          double *dt_out);
 

@@ -142,15 +142,24 @@ def have_ref_gpu() -> bool:
     return os.path.exists(REF_GPU_HARNESS)
 
 
-def ref_run(casedir: str, nsteps: int, cfl: float, dumps, stats_on=True, outdir=None, gpu=False):
+def ref_run(casedir: str, nsteps: int, cfl: float, dumps, stats_on=True, outdir=None, gpu=False, field=False):
     """Run the reference binary (its CPU path, or with gpu=True its GPU path);
-    returns dict(meta, stats, dumps, stdout)."""
+    returns dict(meta, stats, dumps, stdout, field).  With field=True the
+    reference's writeField dumps the primitives once at the first step with
+    t >= t0 into casedir/Results/Field; `field` is then (file name, bytes)."""
     outdir = outdir or tempfile.mkdtemp(prefix="gksref_")
     os.makedirs(outdir, exist_ok=True)
     dl = ",".join(str(d) for d in dumps) if dumps else ","
     cp = subprocess.run([REF_GPU_HARNESS if gpu else REF_HARNESS, "run", os.path.abspath(casedir), os.path.abspath(outdir), str(nsteps),
-                         repr(cfl), "1" if stats_on else "0", dl],
+                         repr(cfl), "1" if stats_on else "0", dl, "1" if field else "0"],
                         check=True, capture_output=True, text=True)
+    fld = None
+    if field:
+        fdir = os.path.join(casedir, "Results", "Field")
+        names = sorted(os.listdir(fdir)) if os.path.isdir(fdir) else []
+        if len(names) == 1:
+            with open(os.path.join(fdir, names[0]), "rb") as f:
+                fld = (names[0], f.read())
     meta = {}
     with open(os.path.join(outdir, "meta.txt")) as f:
         for line in f:
@@ -163,7 +172,7 @@ def ref_run(casedir: str, nsteps: int, cfl: float, dumps, stats_on=True, outdir=
     for d in dumps:
         out[d] = np.fromfile(os.path.join(outdir, f"W_{d}.bin"), dtype=np.float64).reshape(5, nt, nt, nt)
     lines = [ln for ln in cp.stdout.splitlines() if ln.strip() and ln.strip()[0].isdigit()]
-    return {"meta": meta, "stats": st, "dumps": out, "stdout": lines, "outdir": outdir}
+    return {"meta": meta, "stats": st, "dumps": out, "stdout": lines, "outdir": outdir, "field": fld}
 
 
 def _blob(path, n, header: bytes, rows: np.ndarray):

@@ -14,15 +14,22 @@
  * (update.cpp:131-133), HaloTransfer (update.cpp:139-141), t += dt.
  *
  * Modes
- *   run  <casedir> <outdir> <nsteps> <cfl> <stats 0|1> <dumps a,b,..>
+ *   run  <casedir> <outdir> <nsteps> <cfl> <stats 0|1> <dumps a,b,..> [field 0|1]
  *        Reads <casedir>/InitialConditions/{params,Init000}.  cfl <= 0 keeps
  *        the reference's own dt (cfl macro 0.02, param.h:17); cfl > 0 sets
  *        dt = cfl*dx/maxVAL with maxVAL from the reference's timestep().
  *        Writes W_<step>.bin (5 padded arrays), stats.bin (per stats call:
- *        t/t0 TKE Diss SKEWu SKEWv SKEWw KURTu KURTv KURTw), meta.txt.
- *   time <casedir> <nsteps> <slabs> <cfl> [warmup]
- *        Times evolveEulerian + HaloTransfer on the y-slab 0 of a <slabs>x1x1
- *        process grid after [warmup] untimed steps; prints one JSON line.
+ *        t/t0 TKE Diss SKEWu SKEWv SKEWw KURTu KURTv KURTw), meta.txt.  With
+ *        field 1, the reference's writeField (update.cpp:1305-1319) dumps the
+ *        primitives once, at the first step with t >= t0, where Evolve does
+ *        (update.cpp:126-129), into <casedir>/Results/Field/Field_0_<iter>.
+ *   time <casedir> <nsteps> <slabs> <cfl> [warmup] [slab]
+ *        Times evolveEulerian + HaloTransfer on y-slab <slab> (default 0) of a
+ *        <slabs>x1x1 process grid, read from InitialConditions/Init<slab>00
+ *        as the reference's Initialize_DHIT reads a rank's block
+ *        (FlowField.cpp:73-75), after [warmup] untimed steps; prints one
+ *        JSON line.  The single-rank MPI stand-in wraps the slab's own halo,
+ *        so a slab's step does the work of a rank of that grid.
  *   weno <in> <out>   ApplyWENO (update.cpp:502-625) on packed stencils.
  *   flux <in> <out>   flux (GKMflux.cpp:11-215) on packed interface states.
  *
@@ -42,6 +49,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <sys/stat.h>
 #include <unistd.h>
 
 #include "FlowField.h"
@@ -125,13 +133,14 @@ struct Stepper {
 #endif
 };
 
-void setup_block(int slabs)
+void setup_block(int slabs, int slab = 0)
 {
     nprocs = 1;
     procDim[0] = slabs;
     procDim[1] = 1;
     procDim[2] = 1;
-    procId[0] = procId[1] = procId[2] = 0;
+    procId[0] = slab;
+    procId[1] = procId[2] = 0;
     myrank_3d = 0;
     GetParams();
     segment();
@@ -167,6 +176,7 @@ int mode_run(int argc, char **argv)
     const double cfl_run = atof(argv[5]);
     const int do_stats = atoi(argv[6]);
     const std::vector<int> dumps = parse_list(argv[7]);
+    const int do_field = argc > 8 ? atoi(argv[8]) : 0;
     if (chdir(argv[2]) != 0) { perror("chdir"); return 2; }
 
     setup_block(1);
@@ -201,8 +211,20 @@ int mode_run(int argc, char **argv)
             if (d == s) write_padded(outdir + "/W_" + std::to_string(s) + ".bin", W);
     };
 
+    int field_done = 0;
+    auto field = [&]() { // Evolve's one-time dump, update.cpp:126-129
+        if (!do_field || field_done || !(t >= t0)) return;
+        mkdir("Results", 0755);
+        mkdir("Results/Field", 0755);
+        generateSplines(W, splinep, den, u, v, w, p);
+        writeField(den, u, v, w, p);
+        for (int q = 0; q < 5; ++q) destroy_Bspline(splinep[q]);
+        field_done = 1;
+    };
+
     for (int s = 0; s < nsteps; ++s) {
         if (do_stats) stats();
+        field();
         dump(s);
         stepper.step(W);
         halo.exchange(W);
@@ -224,13 +246,15 @@ int mode_run(int argc, char **argv)
 
 int mode_time(int argc, char **argv)
 {
-    if (argc < 6) { fprintf(stderr, "time <casedir> <nsteps> <slabs> <cfl> [warmup]\n"); return 2; }
+    if (argc < 6) { fprintf(stderr, "time <casedir> <nsteps> <slabs> <cfl> [warmup] [slab]\n"); return 2; }
     const int nsteps = atoi(argv[3]);
     const int slabs = atoi(argv[4]);
     const double cfl_run = atof(argv[5]);
     const int warmup = argc > 6 ? atoi(argv[6]) : 0;
+    const int slab = argc > 7 ? atoi(argv[7]) : 0;
+    if (slab < 0 || slab >= slabs) { fprintf(stderr, "slab out of range\n"); return 2; }
     if (chdir(argv[2]) != 0) { perror("chdir"); return 2; }
-    setup_block(slabs);
+    setup_block(slabs, slab);
     ptype *W[5];
     for (int q = 0; q < 5; ++q) W[q] = new ptype[Nt_seg]();
     Stepper stepper;
@@ -257,9 +281,9 @@ int mode_time(int argc, char **argv)
     }
     /* seconds: step + halo exchange; step_seconds: evolveEulerian alone (on the GPU
      * path: evolve, i.e. its host<->device copies and kernels) */
-    printf("{\"cells\": %d, \"nc\": %d, \"slab\": [%d, %d, %d], \"steps\": %d, \"seconds\": %.9g, "
-           "\"step_seconds\": %.9g, \"cell_updates_per_s\": %.9g}\n",
-           Nc_seg, nc, nc_segy, nc_segx, nc_segz, nsteps, tot, tstep, (double)Nc_seg * nsteps / tot);
+    printf("{\"cells\": %d, \"nc\": %d, \"slab\": [%d, %d, %d], \"slab_index\": %d, \"steps\": %d, "
+           "\"seconds\": %.9g, \"step_seconds\": %.9g, \"cell_updates_per_s\": %.9g}\n",
+           Nc_seg, nc, nc_segy, nc_segx, nc_segz, slab, nsteps, tot, tstep, (double)Nc_seg * nsteps / tot);
     return 0;
 }
 

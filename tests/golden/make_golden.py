@@ -16,6 +16,9 @@ Fixtures
                  checksums and 4096 sampled cells
   dhit128.npz    128^3 (same physics, seed 0): 10-step field checksums, 8192 sampled
                  cells, stats history (python make_golden.py --c1; ~3 min of CPU)
+  field8.npz     8^3 DHIT (seed 1, CFL 0.5): the reference's Results/Field text dump
+                 (writeField, update.cpp:1305-1319), written once at the first step
+                 with t >= t0 as Evolve does (python make_golden.py --field)
 """
 
 import hashlib
@@ -129,11 +132,27 @@ def c1():
         mu0=case.mu0, p0=case.p0, t0=case.t0, Mt=case.Mt, seed=0, nc=128, ic_sha256=sha)
 
 
+def field8():
+    """The Results/Field dump of an 8^3 run that passes t = t0."""
+    case = gks_ic.make_dhit(8, seed=1)
+    d = tempfile.mkdtemp(prefix="golden8_")
+    gks_ic.write_case(d, case)
+    dt = pyoracle.ref_run(d, 1, 0.5, [], stats_on=False)["meta"]["dt"]
+    nsteps = int(np.ceil(case.t0 / dt)) + 1
+    r = pyoracle.ref_run(d, nsteps, 0.5, [], stats_on=False, field=True)
+    name, text = r["field"]
+    np.savez_compressed(os.path.join(HERE, "field8.npz"), name=name, text=np.frombuffer(text, dtype=np.uint8),
+                        nsteps=nsteps, dt=dt, seed=1, nc=8)
+
+
 def main():
     if not pyoracle.have_ref():
         pyoracle.build()
     if "--c1" in sys.argv:
         c1()
+        return
+    if "--field" in sys.argv:
+        field8()
         return
     rng = np.random.default_rng(20240601)
 

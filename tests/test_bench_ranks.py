@@ -69,3 +69,29 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_times_the_whole_field():
+    """bench.py --impl reference: one reference process per y-slab, the slabs
+    together the whole field, ms_per_step the slowest process's measured time."""
+    import json
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert bench.reference_slabs(256, 16) == 16
+    assert bench.reference_slabs(256, 6) == 4
+    assert bench.reference_slabs(256, 200) == 64
+    assert bench.reference_slabs(24, 16) == 8
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--nc", "16",
+                        "--steps", "2", "--warmup", "1"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    if "unavailable" in line:
+        pytest.skip(line["unavailable"])
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 1
+    assert line["config"] == bench.bench_config(16, bench.MACH, bench.RE, 1)
+    per = line["per_process_ms_per_step"]
+    assert len(per) == line["cpu_baseline"]["cores"]
+    assert abs(line["ms_per_step"] - max(per)) < 1e-9
+    assert abs(line["value"] - 16 ** 3 / (line["ms_per_step"] * 1e-3)) < 1e-6 * line["value"]

@@ -85,3 +85,76 @@ def test_driver_prints_reference_lines(tmp_path, oracle):
     u = raw[:16**3].reshape(16, 16, 16).transpose(2, 1, 0)
     w10 = g["w10"]
     np.testing.assert_allclose(u, w10[1] / w10[0], rtol=0, atol=1e-12)
+
+
+FIELD_LINE = r"^-?\d+ -?\d+ -?\d+( -?\d\.\d{15}e[+-]\d{2}){5}$"
+
+
+def parse_field(text: str):
+    rows = [ln.split() for ln in text.splitlines()]
+    ijk = np.array([[int(x) for x in r[:3]] for r in rows])
+    vals = np.array([[float(x) for x in r[3:]] for r in rows])
+    return ijk, vals
+
+
+def test_field_golden_is_the_oracle_dump(oracle):
+    """The Results/Field golden (the reference's writeField after 13 steps of
+    the 8^3 case) equals, byte for byte, the same dump formatted from the
+    oracle's state: it pins the fixture on the CPU."""
+    import re
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "field8.npz"))
+    text = g["text"].tobytes().decode()
+    case = gks_ic.make_dhit(8, seed=1)
+    W = gks_ic.to_conservative_padded(case)
+    prm = oracle.params(8, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    dt = 0.5 * (2 * np.pi / 8) / oracle.maxval(W, prm)
+    assert dt == float(g["dt"])
+    # writeField runs at the first step with t >= t0 (update.cpp:126-129), before that step
+    t, n = 0.0, 0
+    while not t >= case.t0:
+        t += dt
+        n += 1
+    assert str(g["name"]) == f"Field_0_{n + 1}" and int(g["nsteps"]) == n + 1
+    oracle.step(W, prm, dt, n)
+    lines = []
+    gam = case.gam
+    for j in range(8):
+        for i in range(8):
+            for k in range(8):
+                w = W[:, j + 3, i + 3, k + 3]
+                d = w[0]
+                u, v, ww = w[1] / d, w[2] / d, w[3] / d
+                vsq = u * u + v * v + ww * ww
+                p = (d * (gam - 1)) * (w[4] / d - 0.5 * vsq)
+                lines.append("%d %d %d %.15e %.15e %.15e %.15e %.15e" % (i, j, k, d, u, v, ww, p))
+    assert "\n".join(lines) + "\n" == text
+    assert all(re.match(FIELD_LINE, ln) for ln in lines)
+
+
+@pytest.mark.gpu
+def test_driver_writes_reference_field(tmp_path):
+    """gks_dns writes the reference's Results/Field dump (writeField,
+    update.cpp:1305-1319): same file name (rank, iteration), same line layout
+    and number format, the same cells in the same order, and primitives equal
+    to the reference's to 1e-12 relative to each column's scale."""
+    import re
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "field8.npz"))
+    ref_text = g["text"].tobytes().decode()
+    case = gks_ic.make_dhit(8, seed=1)
+    gks_ic.write_case(str(tmp_path), case)
+    r = subprocess.run([os.path.join(PKG, "driver", "gks_dns"), "--case", str(tmp_path), "--cfl", "0.5",
+                        "--steps", str(int(g["nsteps"]))], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    fdir = tmp_path / "Results" / "Field"
+    assert sorted(os.listdir(fdir)) == [str(g["name"])]
+    text = (fdir / str(g["name"])).read_text()
+    lines = text.splitlines()
+    assert len(lines) == 8**3 and text.endswith("\n")
+    assert all(re.match(FIELD_LINE, ln) for ln in lines)
+    ijk, vals = parse_field(text)
+    rijk, rvals = parse_field(ref_text)
+    assert np.array_equal(ijk, rijk)
+    scale = np.abs(rvals).max(0)
+    assert np.all(np.abs(vals - rvals).max(0) <= 1e-12 * scale), np.abs(vals - rvals).max(0) / scale

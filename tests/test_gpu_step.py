@@ -99,6 +99,37 @@ def test_fp64_step_matches_reference_32(gks, oracle):
     assert np.all(field_err(W, interior(Wo)) < STEP_RTOL)
 
 
+def test_fp64_stats_history_matches_reference_32(gks):
+    """The CPU configuration (32^3, k0 4, Mt 0.3, Re_lambda 72, seed 0, CFL 0.5)
+    for its full 100 steps: every step's statistics against the reference's
+    PrintStats history (update.cpp:638-784; TKE, dissipation, skewness and
+    kurtosis to 1e-10, the printed p / T / 1/rho rms columns to their 9 printed
+    digits) and the step-100 field sums against the reference's."""
+    g = load("dhit32.npz")
+    case = gks_ic.make_dhit(32, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=0)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(gks_ic.to_conservative_padded(case))
+        dt = s.timestep(0.5)
+        assert dt == float(g["dt"])
+        hist = []
+        for k in range(101):
+            hist.append(s.stats_array())
+            if k < 100:
+                s.step(1)
+        s.sync()
+        W = interior(s.download()).reshape(5, -1)
+    hist = np.array(hist)
+    ref = g["stats"]
+    assert ref.shape == (101, 9)
+    np.testing.assert_allclose(np.arange(101) * dt / case.t0, ref[:, 0], rtol=1e-14, atol=0)
+    np.testing.assert_allclose(hist[:, :8], ref[:, 1:9], rtol=STATS_RTOL, atol=1e-13)
+    printed = np.array([[float(x) for x in str(line).split()] for line in g["lines"]])
+    assert printed.shape == (101, 12)
+    # at t = 0 pressure and density are uniform and their rms columns are round-off
+    np.testing.assert_allclose(hist[1:, 8:11], printed[1:, 9:12], rtol=2e-8, atol=0)
+    np.testing.assert_allclose(W.sum(1), g["sum_w100"], rtol=1e-12, atol=1e-9)
+
+
 def test_fp64_step_matches_reference_128(gks):
     """128^3 (k0 4, Mt 0.3, Re 72, seed 0): 10 steps against the reference's
     own output (sampled cells, per-component sums and sums of squares)."""
@@ -361,6 +392,58 @@ def test_nonfinite_state_is_reported(gks):
         with pytest.raises(gks.GksError) as ei:
             s.check()
         assert ei.value.code == -5
+
+
+def near_vacuum_double_rarefaction(case):
+    """An 8^3 field with one near-vacuum cell (rho 1e-3, p 1e-6) whose x
+    neighbours move away from it at 3x the sound speed: the first step takes
+    more mass out of the cell than it holds, so its density turns negative
+    (-0.068 in the oracle), a finite but unphysical state."""
+    W = gks_ic.to_conservative_padded(case)
+    V = np.ascontiguousarray(W[:, 3:-3, 3:-3, 3:-3])
+    gam = case.gam
+
+    def put(j, i, k, rho, u, p):
+        V[:, j, i, k] = [rho, rho * u, 0.0, 0.0, p / (gam - 1) + 0.5 * rho * u * u]
+
+    put(4, 4, 4, 1e-3, 0.0, 1e-6)
+    put(4, 3, 4, 1.0, -3.0, 1 / gam)
+    put(4, 5, 4, 1.0, 3.0, 1 / gam)
+    return gks_ic.pad_periodic(V)
+
+
+def test_step_that_breaks_the_state_is_reported(gks, oracle):
+    """The update kernel's error word: a step that leaves a non-positive density
+    or pressure makes gks_sync return GKS_ENONFINITE (no GPU fault: the state is
+    finite but unphysical), gks_check then finds it too, and the context keeps
+    working after a fresh upload."""
+    case = gks_ic.make_dhit(8, seed=0)
+    bad = near_vacuum_double_rarefaction(case)
+    # the checker agrees that one step breaks this state
+    prm = oracle.params(8, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    dt = 0.5 * (2 * np.pi / 8) / oracle.maxval(bad, prm)
+    ref = bad.copy()
+    oracle.step(ref, prm, dt, 1)
+    assert interior(ref)[0].min() < -1e-2
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(bad)
+        s.check()  # the uploaded state itself is physical
+        assert s.timestep(0.5) == dt
+        s.step(1)
+        with pytest.raises(gks.GksError) as ei:
+            s.sync()
+        assert ei.value.code == -5
+        with pytest.raises(gks.GksError) as ei:
+            s.check()
+        assert ei.value.code == -5
+        # the error word was cleared by the sync that reported it; a good state runs on
+        good = gks_ic.to_conservative_padded(case)
+        s.upload(good)
+        s.check()
+        s.timestep(0.5)
+        s.step(2)
+        s.sync()
+        s.check()
 
 
 def test_call_order_is_enforced(gks):

@@ -75,6 +75,18 @@ def test_slab_case_holds_first_planes(tmp_path):
     assert raw.size == 5 * 2 * 64
 
 
+def test_all_slabs_tile_the_field(tmp_path):
+    """Init<a>00 holds y-planes [2a, 2a+2): the slabs together are the whole field."""
+    case = gks_ic.make_dhit(8, seed=1)
+    gks_ic.write_case(str(tmp_path), case, slab_planes=2, all_slabs=True)
+    for a in range(4):
+        raw = np.fromfile(str(tmp_path / "InitialConditions" / f"Init{a}00"), dtype="<f8").reshape(5, 8, 8, 2)
+        # file order: k slowest, then i, then j (FlowField.cpp:95)
+        u = raw[0].transpose(2, 1, 0)
+        assert np.array_equal(u, case.u[2 * a:2 * a + 2])
+        assert np.array_equal(raw[3].transpose(2, 1, 0), case.rho[2 * a:2 * a + 2])
+
+
 def _header_symbols():
     with open(os.path.join(ROOT, "include", "gks_b200.h")) as f:
         text = f.read()
