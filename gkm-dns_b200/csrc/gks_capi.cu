@@ -30,6 +30,11 @@ struct FieldHost {
     FieldDev dev;
     double *mem = nullptr;
     double *spl = nullptr;
+    // slab-pipelined host step (gks_evolve): one allocation of 25 nc^3 doubles
+    // -- the spare state the step writes (5) and the y and z sweeps' own
+    // reconstruction buffers (10 + 10) -- made on first use
+    double *pipe = nullptr;
+    double *spare[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool uploaded = false;
     bool have_dt = false;
 };
@@ -50,6 +55,12 @@ struct gks_ctx {
     cudaGraphExec_t graph = nullptr;
     double *d_stage = nullptr;
     size_t stage_elems = 0;
+    // gks_evolve: the padded staging of the downloaded state, the copy streams
+    // and one event per slab and direction
+    double *d_stage_out = nullptr;
+    size_t stage_out_elems = 0;
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    std::vector<cudaEvent_t> ev_in, ev_out;
     double *d_partial = nullptr;
     double *d_sums = nullptr;
     unsigned long long *d_bits = nullptr;
@@ -215,6 +226,209 @@ int build_graph(gks_ctx *ctx)
     return GKS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Slab-pipelined host step (gks_evolve, one field, one step): the padded host
+// state goes up in y-slabs on one copy stream, each slab's reconstruction,
+// flux and update stages run on the context's stream as soon as the planes
+// they read are on the device, and the updated planes come back on a second
+// copy stream, so that the two PCIe directions and the step overlap.
+//
+// Planes are counted in an unwrapped y coordinate u in [-3, nc - 3) (plane
+// u mod nc), uploaded in increasing u: first the three planes below 0 (nc-3
+// .. nc-1), then slabs of about nc / kPipeSlabs planes.  With F the uploaded
+// frontier, the stages advance as far as the planes they read allow (each
+// stage covers every plane once):
+//   x, z reconstruction  u in [-3, nc-3)   needs W(u)                    u < F
+//   x, z flux            u in [-2, nc-2)   needs rec(u-1 .. u+1)         u < rec - 1
+//   y reconstruction     u in [-1, nc-1)   needs W(u-2 .. u+3)           u < F - 3
+//   y flux               u in [-1, nc-1)   needs rec_y(u), W(u+1), mu/p  u < rec_y, rec
+//   update               u in [0, nc)      needs Fx, Fz (u), Fy(u-1, u)
+// and every stage completes after the last slab.  Ranges that wrap past a
+// stage's end are deferred to completion, so no stage reads a plane before it
+// exists.  The update writes the new state into a spare buffer (the old state
+// is still read by later slabs' stencils); afterwards the two swap.  The
+// sweeps keep separate reconstruction buffers, as their slabs interleave.
+// ---------------------------------------------------------------------------
+constexpr int kPipeSlabs = 16;
+constexpr int kPipeMinNc = 16;
+
+int ensure_pipe(gks_ctx *ctx, FieldHost &h)
+{
+    const size_t n = (size_t)h.phys.nc * h.phys.nc * h.phys.nc;
+    if (!h.pipe) {
+        if (cudaMalloc(&h.pipe, 25 * n * sizeof(double)) != cudaSuccess) {
+            h.pipe = nullptr;
+            return fail(ctx, GKS_ENOMEM, "pipelined-step buffers allocation failed");
+        }
+        for (int q = 0; q < 5; ++q) h.spare[q] = h.pipe + q * n;
+    }
+    const size_t nt = (size_t)h.phys.nc + 6, need = 5 * nt * nt * nt;
+    if (ctx->stage_out_elems < need) {
+        if (ctx->d_stage_out) cudaFree(ctx->d_stage_out);
+        ctx->d_stage_out = nullptr;
+        ctx->stage_out_elems = 0;
+        if (cudaMalloc(&ctx->d_stage_out, need * sizeof(double)) != cudaSuccess)
+            return fail(ctx, GKS_ENOMEM, "download staging allocation failed");
+        ctx->stage_out_elems = need;
+    }
+    if (!ctx->h2d) CK(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+    if (!ctx->d2h) CK(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+    while ((int)ctx->ev_in.size() < kPipeSlabs + 2) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->ev_in.push_back(e);
+    }
+    while ((int)ctx->ev_out.size() < kPipeSlabs + 2) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->ev_out.push_back(e);
+    }
+    return GKS_OK;
+}
+
+// One stage over the physical planes [p0, p1) of the single field.
+int pipe_stage(gks_ctx *ctx, const FieldDev &d, int kind, int dir, long long p0, long long p1)
+{
+    if (p1 <= p0) return GKS_OK;
+    const long long nc = d.nc;
+    gks::Batch b = ctx->batch;
+    gks::LaunchCfg c = ctx->cfg[kind][dir];
+    long long per_plane = nc * nc; // cells
+    if (kind == gks::K_RECON && c.variant < 3) {
+        if (dir == 0) per_plane = (long long)d.nrun * nc; // window items (j, run, k)
+        else if (dir == 2) per_plane = nc * ((nc + 31) / 32); // z segments ((j, i), segment)
+        else c = persistent(ctx, kind, dir, c.variant + 3, 1); // y windows run along y: one interface per thread
+    }
+    b.lo = p0 * per_plane;
+    b.hi = p1 * per_plane;
+    if (kind == gks::K_RECON) CK(gks::launch_recon(b, dir, ctx->precision, c, ctx->stream));
+    else if (kind == gks::K_FLUX) CK(gks::launch_flux(b, dir, ctx->precision, c, ctx->stream));
+    else CK(gks::launch_update(b, c, ctx->stream));
+    return GKS_OK;
+}
+
+int evolve_pipelined(gks_ctx *ctx, double *const W[5])
+{
+    FieldHost &h = ctx->fh[0];
+    int rc = ensure_stage(ctx, 0);
+    if (!rc) rc = ensure_pipe(ctx, h);
+    if (rc) return rc;
+    const long long nc = h.phys.nc, nt = nc + 6, P = nt * nt, Nt = P * nt, plane = nc * nc;
+    // descriptor of this step: reads the uploaded state, writes the spare,
+    // the y and z sweeps into their own reconstruction buffers
+    FieldDev d = h.dev;
+    const size_t n = (size_t)nc * nc * nc;
+    for (int q = 0; q < 5; ++q) d.Wout[q] = h.spare[q];
+    for (int q = 0; q < 10; ++q) {
+        d.rec[1][q] = h.pipe + (5 + q) * n;
+        d.rec[2][q] = h.pipe + (15 + q) * n;
+    }
+    CK(cudaMemcpyAsync(ctx->d_fields, &d, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream)); // the h2d stream writes the stage the last call may still read
+
+    // slabs in unwrapped planes: [-3, 0), then [(k-1) S, min(k S, nc-3))
+    const long long S = (nc - 3 + kPipeSlabs - 1) / kPipeSlabs;
+    std::vector<std::pair<long long, long long>> slabs{{-3, 0}};
+    for (long long a = 0; a < nc - 3; a += S) slabs.push_back({a, std::min(a + S, nc - 3)});
+    struct Cur {
+        long long done, end;
+    };
+    Cur rec{-3, nc - 3}, flx{-2, nc - 2}, recy{-1, nc - 1}, fly{-1, nc - 1}, upd{0, nc};
+    // run fn over the physical planes of unwrapped [a, b)
+    auto phys = [&](long long a, long long b, auto fn) -> int {
+        int r = GKS_OK;
+        if (a < b && a < 0 && !r) r = fn(a + nc, std::min(b, 0LL) + nc);
+        if (a < b && b > 0 && !r) r = fn(std::max(a, 0LL), b);
+        return r;
+    };
+    auto advance = [&](Cur &c, long long ready, auto fn) -> int {
+        ready = std::min(ready, c.end);
+        if (ready <= c.done) return GKS_OK;
+        const int r = phys(c.done, ready, fn);
+        c.done = ready;
+        return r;
+    };
+    std::vector<std::pair<long long, long long>> out_planes; // physical planes downloaded after slab k
+    for (size_t k = 0; k < slabs.size(); ++k) {
+        const long long a = slabs[k].first, b = slabs[k].second;
+        const bool all = k + 1 == slabs.size();
+        // upload: padded planes of unwrapped [a, b) (physical planes + 3), one copy per component
+        int r = phys(a, b, [&](long long p0, long long p1) -> int {
+            for (int q = 0; q < 5; ++q)
+                CK(cudaMemcpyAsync(ctx->d_stage + q * Nt + (p0 + 3) * P, W[q] + (p0 + 3) * P,
+                                   (size_t)(p1 - p0) * P * sizeof(double), cudaMemcpyHostToDevice, ctx->h2d));
+            return GKS_OK;
+        });
+        if (r) return r;
+        CK(cudaEventRecord(ctx->ev_in[k], ctx->h2d));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[k], 0));
+        r = phys(a, b, [&](long long p0, long long p1) -> int {
+            CK(gks::launch_gather(d, ctx->d_stage, ctx->nsm, ctx->stream, p0 * plane, p1 * plane));
+            return GKS_OK;
+        });
+        if (r) return r;
+        const long long F = b;
+        auto st = [&](int kind, int dir) {
+            return [&, kind, dir](long long p0, long long p1) { return pipe_stage(ctx, d, kind, dir, p0, p1); };
+        };
+        auto two = [&](int kind, int d0, int d1) {
+            return [&, kind, d0, d1](long long p0, long long p1) {
+                int e = pipe_stage(ctx, d, kind, d0, p0, p1);
+                return e ? e : pipe_stage(ctx, d, kind, d1, p0, p1);
+            };
+        };
+        if ((r = advance(rec, all ? rec.end : F, two(gks::K_RECON, 0, 2)))) return r;
+        if ((r = advance(flx, rec.done == rec.end ? flx.end : rec.done - 1, two(gks::K_FLUX, 0, 2)))) return r;
+        if ((r = advance(recy, all ? recy.end : F - 3, st(gks::K_RECON, 1)))) return r;
+        if ((r = advance(fly, std::min(recy.done, rec.done == rec.end ? fly.end : rec.done), st(gks::K_FLUX, 1))))
+            return r;
+        const long long u0 = upd.done;
+        const long long rx = flx.done == flx.end ? upd.end : flx.done;
+        const long long ry = fly.done == fly.end ? upd.end : fly.done;
+        if ((r = advance(upd, std::min(rx, ry), st(gks::K_UPDATE, 0)))) return r;
+        // the updated planes, with their i / k ghosts, into the download staging
+        FieldDev dn = d;
+        for (int q = 0; q < 5; ++q) dn.W[q] = d.Wout[q];
+        const long long u1 = upd.done;
+        if (u1 > u0) CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, (u0 + 3) * P, (u1 + 3) * P));
+        if (all) { // the y ghost planes: the periodic images of planes nc-3 .. nc-1 and 0 .. 2
+            CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, 0, 3 * P));
+            CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, (nt - 3) * P, Nt));
+        }
+        CK(cudaEventRecord(ctx->ev_out[k], ctx->stream));
+        out_planes.push_back({u0 + 3, u1 + 3});
+    }
+    // downloads, each after its slab's update (enqueued after all uploads and
+    // stages, so that a blocking copy into pageable memory holds up nothing)
+    for (size_t k = 0; k < out_planes.size(); ++k) {
+        CK(cudaStreamWaitEvent(ctx->d2h, ctx->ev_out[k], 0));
+        std::vector<std::pair<long long, long long>> rng{out_planes[k]};
+        if (k + 1 == out_planes.size()) {
+            rng.push_back({0, 3});
+            rng.push_back({nt - 3, nt});
+        }
+        for (auto pr : rng) {
+            if (pr.second <= pr.first) continue;
+            for (int q = 0; q < 5; ++q)
+                CK(cudaMemcpyAsync(W[q] + pr.first * P, ctx->d_stage_out + q * Nt + pr.first * P,
+                                   (size_t)(pr.second - pr.first) * P * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->d2h));
+        }
+    }
+    CK(cudaEventRecord(ctx->ev_in[slabs.size()], ctx->d2h));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[slabs.size()], 0));
+    // the new state is the spare: swap, so that the field's descriptor names it
+    for (int q = 0; q < 5; ++q) {
+        double *old = h.dev.W[q];
+        h.dev.W[q] = h.dev.Wout[q] = h.spare[q];
+        h.spare[q] = old;
+    }
+    CK(cudaMemcpyAsync(ctx->d_fields, &h.dev, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    h.uploaded = true;
+    return GKS_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -269,8 +483,9 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         if (cudaMemset(h.mem, 0, (size_t)32 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ECUDA);
         FieldDev &d = h.dev;
         memset(&d, 0, sizeof(d));
-        for (int q = 0; q < 5; ++q) d.W[q] = h.mem + q * n;
-        for (int q = 0; q < 10; ++q) d.rec[q] = h.mem + (5 + q) * n;
+        for (int q = 0; q < 5; ++q) d.W[q] = d.Wout[q] = h.mem + q * n;
+        for (int sw = 0; sw < 3; ++sw)
+            for (int q = 0; q < 10; ++q) d.rec[sw][q] = h.mem + (5 + q) * n;
         for (int q = 0; q < 15; ++q) d.F[q] = h.mem + (15 + q) * n;
         for (int q = 0; q < 2; ++q) d.tau[q] = h.mem + (30 + q) * n;
         const int nt = p.nc + 6;
@@ -355,9 +570,15 @@ void gks_destroy(gks_ctx *ctx)
     for (FieldHost &h : ctx->fh) {
         if (h.mem) cudaFree(h.mem);
         if (h.spl) cudaFree(h.spl);
+        if (h.pipe) cudaFree(h.pipe);
     }
     if (ctx->d_fields) cudaFree(ctx->d_fields);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->d_stage_out) cudaFree(ctx->d_stage_out);
+    for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->ev_out) cudaEventDestroy(e);
+    if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
+    if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
     if (ctx->d_partial) cudaFree(ctx->d_partial);
     if (ctx->d_sums) cudaFree(ctx->d_sums);
     if (ctx->d_bits) cudaFree(ctx->d_bits);
@@ -399,6 +620,25 @@ int gks_download(gks_ctx *ctx, int f, double *const W[5])
         CK(cudaMemcpyAsync(W[q], ctx->d_stage + q * Nt, Nt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return GKS_OK;
+}
+
+int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    if (!W) return fail(ctx, GKS_EINVAL, "null field pointer");
+    for (int q = 0; q < 5; ++q)
+        if (!W[q]) return fail(ctx, GKS_EINVAL, "null component pointer");
+    if (nsteps < 1) return fail(ctx, GKS_EINVAL, "nsteps must be at least 1");
+    if (!ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "evolve before dt of field " + std::to_string(f));
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->nfields == 1 && nsteps == 1 && ctx->fh[f].phys.nc >= kPipeMinNc) return evolve_pipelined(ctx, W);
+    // several fields or steps: upload, the captured steps, download
+    if ((rc = gks_upload(ctx, f, W))) return rc;
+    for (int g = 0; g < ctx->nfields; ++g)
+        if (!ctx->fh[g].uploaded) return fail(ctx, GKS_ESTATE, "evolve with field " + std::to_string(g) + " not uploaded");
+    if ((rc = gks_step(ctx, nsteps))) return rc;
+    return gks_download(ctx, f, W);
 }
 
 int gks_set_dt(gks_ctx *ctx, int f, double dt)

@@ -205,7 +205,7 @@ template <int DIR, int PREC, int MINB>
 __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
+    for (long long it = b.lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.hi; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
         if (it - f.base >= f.ncell) continue; // alignment padding after the field
         const Cell x = decode(unsigned(it - f.base), f);
@@ -228,8 +228,8 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
         recon_point<PREC>(s, T, direct, f.icT, wl, wr);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            f.rec[q][x.c] = wl[q];
-            f.rec[5 + q][x.c] = wr[q];
+            f.rec[DIR][q][x.c] = wl[q];
+            f.rec[DIR][5 + q][x.c] = wr[q];
         }
     }
 }
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_zseg(Batch b)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double (*tile)[kZSegCells] = tiles[wid];
     const long long stride = (long long)gridDim.x * kZSegWarps;
-    for (long long it = (long long)blockIdx.x * kZSegWarps + wid; it < b.ztotal; it += stride) {
+    for (long long it = b.lo + (long long)blockIdx.x * kZSegWarps + wid; it < b.hi; it += stride) {
         const FieldDev &f = b.fields[field_of_zseg(b.fields, b.nfields, it)];
         const long long loc = it - f.zbase; // < nzseg: segment ranges are contiguous
         const int nc = f.nc, nseg = (nc + 31) >> 5;
@@ -325,8 +325,8 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_zseg(Batch b)
             const unsigned c = lbase + unsigned(k);
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                f.rec[q][c] = wl[q];
-                f.rec[5 + q][c] = wr[q];
+                f.rec[2][q][c] = wl[q];
+                f.rec[2][5 + q][c] = wr[q];
             }
         }
         __syncwarp();
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
     const int tid = threadIdx.x;
     static_assert(DIR == 0 || DIR == 1, "windowed reconstruction is for the x and y sweeps");
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.wtotal; it += stride) {
+    for (long long it = b.lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.hi; it += stride) {
         const FieldDev &f = b.fields[field_of_win(b.fields, b.nfields, it)];
         const long long loc = it - f.wbase;
         if (loc >= f.nwin) continue; // alignment padding after the field
@@ -435,8 +435,8 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
             }
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                f.rec[q][c] = wl[q];
-                f.rec[5 + q][c] = wr[q];
+                f.rec[DIR][q][c] = wl[q];
+                f.rec[DIR][5 + q][c] = wr[q];
             }
             // cell p + 3 + PF takes the slot of cell p + 3 + PF - NR, which no
             // stencil from here on reads (it lies below p - 2 for NR >= 5 + PF)
@@ -508,7 +508,7 @@ struct SweepSrc {
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             const int o = perm(q);
-            const double *rl = f.rec[o], *rr = f.rec[5 + o];
+            const double *rl = f.rec[DIR][o], *rr = f.rec[DIR][5 + o];
             const double wL = __ldg(f.W[o] + c), wR = __ldg(f.W[o] + c1);
             const double wr = __ldg(rr + c);
             Wl[q] = __ldg(rl + c);
@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
     __shared__ double sum_d[10][kFluxBlock];
     __shared__ S sum_s[20][kFluxBlock];
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
+    for (long long it = b.lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.hi; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
         if (it - f.base >= f.ncell) continue; // alignment padding after the field
         const Cell x = decode(unsigned(it - f.base), f);
@@ -614,13 +614,14 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
 
 // ---------------------------------------------------------------------------
 // Conservative update of the interior (update.cpp:455-469), evaluated in the
-// reference's order: W - (1/dx)*(Fx - Fx[i-1] + Fy - Fy[j-1] + Fz - Fz[k-1]).
-// Also flags non-finite or non-positive density / pressure.
+// reference's order: W - (1/dx)*(Fx - Fx[i-1] + Fy - Fy[j-1] + Fz - Fz[k-1]),
+// written to Wout (W itself, except in the slab-pipelined host step).  Also
+// flags non-finite or non-positive density / pressure.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kUpdateBlock) k_update(Batch b)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.total; it += stride) {
+    for (long long it = b.lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.hi; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
         if (it - f.base >= f.ncell) continue; // alignment padding after the field
         const Cell x = decode(unsigned(it - f.base), f);
@@ -635,7 +636,7 @@ __global__ void __launch_bounds__(kUpdateBlock) k_update(Batch b)
             d = __dadd_rn(d, f.F[10 + q][c]);
             d = __dsub_rn(d, f.F[10 + q][cz]);
             w[q] = __dsub_rn(f.W[q][c], __dmul_rn(f.inv_dx, d));
-            f.W[q][c] = w[q];
+            f.Wout[q][c] = w[q];
         }
         const double p = f.gm1 * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) / w[0]);
         if (!(w[0] > 0.0) || !(p > 0.0) || !isfinite(w[0] + w[1] + w[2] + w[3] + w[4]))
@@ -646,12 +647,12 @@ __global__ void __launch_bounds__(kUpdateBlock) k_update(Batch b)
 // ---------------------------------------------------------------------------
 // Layout conversion: padded staging (5 x nt^3) <-> interior.
 // ---------------------------------------------------------------------------
-__global__ void k_gather(FieldDev f, const double *__restrict__ stage)
+__global__ void k_gather(FieldDev f, const double *__restrict__ stage, long long lo, long long hi)
 {
     const int nc = f.nc, nt = nc + 6;
     const long long Nt = (long long)nt * nt * nt;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
+    for (long long c = lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; c < hi; c += stride) {
         const Cell x = decode(unsigned(c), f);
         const long long p = ((long long)(x.j + 3) * nt + (x.i + 3)) * nt + (x.k + 3);
 #pragma unroll
@@ -659,12 +660,12 @@ __global__ void k_gather(FieldDev f, const double *__restrict__ stage)
     }
 }
 
-__global__ void k_scatter(FieldDev f, double *__restrict__ stage)
+__global__ void k_scatter(FieldDev f, double *__restrict__ stage, long long lo, long long hi)
 {
     const int nc = f.nc, nt = nc + 6;
     const long long Nt = (long long)nt * nt * nt;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < Nt; p += stride) {
+    for (long long p = lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += stride) {
         const int kk = int(p % nt);
         const int ii = int((p / nt) % nt);
         const int jj = int(p / ((long long)nt * nt));
@@ -1054,41 +1055,67 @@ cudaError_t occ(KernelT k, int block, int *n)
 constexpr int kReconMinb[3] = {3, 4, 5};
 constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
 
+// The item range of a launch (all items of its kind when b.hi < 0) and the
+// blocks it needs: at most cfg.grid, no more than the range fills.
+Batch resolve_range(Batch b, int kind, int dir, int variant)
+{
+    if (b.hi < 0) {
+        b.lo = 0;
+        b.hi = batch_items(b, kind, dir, variant);
+    }
+    return b;
+}
+
+int range_grid(int grid, long long items, int items_per_block)
+{
+    const long long need = (items + items_per_block - 1) / items_per_block;
+    return int(std::max(1LL, std::min((long long)grid, need)));
+}
+
 // Reconstruction variants: 0-2 the windowed kernel (x, y sweeps) or the
 // warp-staged segment kernel (z sweep) at the three register caps, 3-5 the
 // one-interface-per-thread kernel at the same caps.
 template <int DIR, int PREC>
-cudaError_t recon_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
+cudaError_t recon_go(Batch b, LaunchCfg cfg, cudaStream_t st)
 {
+    b = resolve_range(b, K_RECON, DIR, cfg.variant);
+    if (b.hi <= b.lo) return cudaSuccess;
+    const long long items = b.hi - b.lo;
     if (DIR < 2 && cfg.variant < 3) {
+        const int g = range_grid(cfg.grid, items, cfg.block);
         switch (cfg.variant) {
-        case 1: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        case 2: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        default: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 1: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[1]><<<g, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[2]><<<g, cfg.block, 0, st>>>(b); break;
+        default: k_recon_win<DIR < 2 ? DIR : 0, PREC, kReconMinb[0]><<<g, cfg.block, 0, st>>>(b); break;
         }
     } else if (DIR == 2 && cfg.variant < 3) {
+        const int g = range_grid(cfg.grid, items, kZSegWarps);
         switch (cfg.variant) {
-        case 1: k_recon_zseg<PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        case 2: k_recon_zseg<PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        default: k_recon_zseg<PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 1: k_recon_zseg<PREC, kReconMinb[1]><<<g, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon_zseg<PREC, kReconMinb[2]><<<g, cfg.block, 0, st>>>(b); break;
+        default: k_recon_zseg<PREC, kReconMinb[0]><<<g, cfg.block, 0, st>>>(b); break;
         }
     } else {
+        const int g = range_grid(cfg.grid, items, cfg.block);
         switch (cfg.variant % 3) {
-        case 1: k_recon<DIR, PREC, kReconMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        case 2: k_recon<DIR, PREC, kReconMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-        default: k_recon<DIR, PREC, kReconMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+        case 1: k_recon<DIR, PREC, kReconMinb[1]><<<g, cfg.block, 0, st>>>(b); break;
+        case 2: k_recon<DIR, PREC, kReconMinb[2]><<<g, cfg.block, 0, st>>>(b); break;
+        default: k_recon<DIR, PREC, kReconMinb[0]><<<g, cfg.block, 0, st>>>(b); break;
         }
     }
     return cudaGetLastError();
 }
 
 template <int DIR, int PREC>
-cudaError_t flux_go(const Batch &b, LaunchCfg cfg, cudaStream_t st)
+cudaError_t flux_go(Batch b, LaunchCfg cfg, cudaStream_t st)
 {
+    b = resolve_range(b, K_FLUX, DIR, cfg.variant);
+    if (b.hi <= b.lo) return cudaSuccess;
+    const int g = range_grid(cfg.grid, b.hi - b.lo, cfg.block);
     switch (cfg.variant) {
-    case 1: k_flux<DIR, PREC, kFluxMinb[1]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-    case 2: k_flux<DIR, PREC, kFluxMinb[2]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
-    default: k_flux<DIR, PREC, kFluxMinb[0]><<<cfg.grid, cfg.block, 0, st>>>(b); break;
+    case 1: k_flux<DIR, PREC, kFluxMinb[1]><<<g, cfg.block, 0, st>>>(b); break;
+    case 2: k_flux<DIR, PREC, kFluxMinb[2]><<<g, cfg.block, 0, st>>>(b); break;
+    default: k_flux<DIR, PREC, kFluxMinb[0]><<<g, cfg.block, 0, st>>>(b); break;
     }
     return cudaGetLastError();
 }
@@ -1138,9 +1165,11 @@ cudaError_t launch_flux(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaSt
     return dir == 0 ? flux_go<0, 1>(b, cfg, st) : dir == 1 ? flux_go<1, 1>(b, cfg, st) : flux_go<2, 1>(b, cfg, st);
 }
 
-cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st)
+cudaError_t launch_update(const Batch &batch, LaunchCfg cfg, cudaStream_t st)
 {
-    k_update<<<cfg.grid, cfg.block, 0, st>>>(b);
+    const Batch b = resolve_range(batch, K_UPDATE, 0, 0);
+    if (b.hi <= b.lo) return cudaSuccess;
+    k_update<<<range_grid(cfg.grid, b.hi - b.lo, cfg.block), cfg.block, 0, st>>>(b);
     return cudaGetLastError();
 }
 
@@ -1150,16 +1179,20 @@ cudaError_t max_resident_blocks(int kind, int dir, int prec, int variant, int bl
     return prec == 0 ? occ_dir<0>(kind, dir, variant, block, n) : occ_dir<1>(kind, dir, variant, block, n);
 }
 
-cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaStream_t st)
+cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaStream_t st, long long lo, long long hi)
 {
-    k_gather<<<helper_grid(f.ncell, 256, nsm), 256, 0, st>>>(f, stage);
+    if (hi < 0) hi = f.ncell;
+    if (hi <= lo) return cudaSuccess;
+    k_gather<<<helper_grid(hi - lo, 256, nsm), 256, 0, st>>>(f, stage, lo, hi);
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st)
+cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st, long long lo, long long hi)
 {
     const long long nt = f.nc + 6;
-    k_scatter<<<helper_grid(nt * nt * nt, 256, nsm), 256, 0, st>>>(f, stage);
+    if (hi < 0) hi = nt * nt * nt;
+    if (hi <= lo) return cudaSuccess;
+    k_scatter<<<helper_grid(hi - lo, 256, nsm), 256, 0, st>>>(f, stage, lo, hi);
     return cudaGetLastError();
 }
 

@@ -5,8 +5,9 @@
 // index (j*nc + i)*nc + k, j = y, i = x, k = z), the periodic halo being
 // applied by index wrapping inside the kernels.  Per field the context also
 // holds a reconstruction buffer (10 arrays: the left and right WENO states of
-// the interface at the high side of every cell, for the sweep in progress)
-// and a flux buffer (15 arrays: the x, y and z interface fluxes of the step).
+// the interface at the high side of every cell, for the sweep in progress;
+// the slab-pipelined host step gives each sweep its own 10 arrays) and a flux
+// buffer (15 arrays: the x, y and z interface fluxes of the step).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,7 +19,8 @@ namespace gks {
 
 struct FieldDev {
     double *W[5];     // state, interior layout
-    double *rec[10];  // Wl[0..4], Wr[0..4] of the current sweep
+    double *Wout[5];  // where the update writes the new state: W itself, except in the slab-pipelined host step
+    double *rec[3][10]; // per sweep x, y, z: Wl[0..4], Wr[0..4] (one shared buffer except in the pipelined step)
     double *F[15];    // Fx[0..4], Fy[0..4], Fz[0..4]
     double *tau[2];   // mu/p of each cell as numerator / denominator, set by the x-sweep reconstruction
     const double *spl_cp;   // natural-spline Thomas coefficients, nt entries
@@ -63,6 +65,9 @@ struct Batch {
     long long wtotal; // end of the last field's window item range
     long long ztotal; // end of the last field's z-segment item range
     int *err;         // device error word (bit 0: non-finite / non-positive state after update)
+    // work items a launch processes: [lo, hi) of the launched kernel's item
+    // space; hi < 0 means all of them (the launchers fill the range in)
+    long long lo = 0, hi = -1;
 };
 
 // Launch configuration chosen by the tuner per kernel kind and sweep: block
@@ -82,7 +87,18 @@ constexpr int kReconBlock = 128;
 constexpr int kFluxBlock = 64;
 constexpr int kUpdateBlock = 256;
 
-// Stage launchers (asynchronous on `st`).  prec: 0 FP64, 1 mixed.
+// Work items of a kernel kind / sweep / variant over the whole batch: window
+// runs (x / y reconstruction variants 0-2), z segments of one warp each (z
+// reconstruction variants 0-2), else cells.
+inline long long batch_items(const Batch &b, int kind, int dir, int variant)
+{
+    if (kind == K_RECON && variant < 3) return dir < 2 ? b.wtotal : b.ztotal;
+    return b.total;
+}
+
+// Stage launchers (asynchronous on `st`).  prec: 0 FP64, 1 mixed.  Each
+// processes the items [b.lo, b.hi) (all items when b.hi < 0) with at most
+// cfg.grid blocks.
 cudaError_t launch_recon(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);
 cudaError_t launch_flux(const Batch &b, int dir, int prec, LaunchCfg cfg, cudaStream_t st);
 cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st);
@@ -91,8 +107,13 @@ cudaError_t launch_update(const Batch &b, LaunchCfg cfg, cudaStream_t st);
 cudaError_t max_resident_blocks(int kind, int dir, int prec, int variant, int block, int *blocks_per_sm);
 
 // Layout conversion of one field: padded host layout (5 x nt^3, contiguous) <-> interior.
-cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaStream_t st);
-cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st);
+// gather fills the interior cells [lo, hi) of f.W (hi < 0: all); scatter fills
+// the padded cells [lo, hi) of `stage` (hi < 0: all) from f.W, ghosts as the
+// periodic image.
+cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaStream_t st, long long lo = 0,
+                          long long hi = -1);
+cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st, long long lo = 0,
+                           long long hi = -1);
 
 // max(|u| + c) over the interior of one field into *out_bits (uint64 image of a positive double;
 // *out_bits must be zero on entry).

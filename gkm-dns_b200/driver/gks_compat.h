@@ -15,9 +15,11 @@
 //   GKS_COMPAT_GPU_SEMANTICS  reproduce the reference GPU kernel's choices
 //                             (WENO on rho E, no 1/Pr factor) instead of the
 //                             CPU path's (the parity default)
-// As in the reference, evolve() uploads W, advances one step and downloads W;
-// the downloaded ghosts already hold the periodic image, so the caller's
-// HaloTransfer that follows leaves them unchanged.
+// As in the reference, evolve() uploads W, advances one step and downloads W
+// (gks_evolve: the copies overlap the step slab by slab; with W in pinned host
+// memory both PCIe directions and the step run concurrently); the downloaded
+// ghosts already hold the periodic image, so the caller's HaloTransfer that
+// follows leaves them unchanged.
 #pragma once
 
 #include <cstdio>
@@ -80,9 +82,7 @@ inline DevAlloc::DevAlloc()
 
 inline void evolve(ptype *W[5], DevAlloc *dev, ptype dt)
 {
-    gks_compat_check(dev->ctx, gks_upload(dev->ctx, 0, W), "gks_upload");
     gks_compat_check(dev->ctx, gks_set_dt(dev->ctx, 0, dt), "gks_set_dt");
-    gks_compat_check(dev->ctx, gks_step(dev->ctx, 1), "gks_step");
+    gks_compat_check(dev->ctx, gks_evolve(dev->ctx, 0, W, 1), "gks_evolve");
     gks_compat_check(dev->ctx, gks_sync(dev->ctx), "gks_sync");
-    gks_compat_check(dev->ctx, gks_download(dev->ctx, 0, W), "gks_download");
 }

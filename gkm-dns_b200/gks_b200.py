@@ -74,6 +74,7 @@ SIGNATURES = {
     "gks_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gks_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
     "gks_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
+    "gks_evolve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5, ctypes.c_int]),
     "gks_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, DP]),
     "gks_set_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]),
     "gks_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -204,6 +205,17 @@ class Solver:
             out = np.empty((5, nt, nt, nt))
         self._ck(self._lib.gks_download(self._h, f, _ptrs(out)))
         return out
+
+    def evolve(self, W: np.ndarray, nsteps: int = 1, f: int = 0) -> np.ndarray:
+        """The reference's per-step call on host memory: W (5, nt, nt, nt) is
+        uploaded, advanced nsteps steps and overwritten with the result (ghosts
+        as the periodic image).  One field and one step overlap the copies with
+        the step; pass W in pinned memory for full overlap."""
+        nt = self.fields[f].nc + 6
+        if W.shape != (5, nt, nt, nt) or W.dtype != np.float64 or not W.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"expected a C-contiguous float64 array of shape {(5, nt, nt, nt)}")
+        self._ck(self._lib.gks_evolve(self._h, f, _ptrs(W), nsteps))
+        return W
 
     def timestep(self, cfl: float, f: int = 0) -> float:
         dt = ctypes.c_double()

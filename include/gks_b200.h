@@ -105,6 +105,20 @@ const char *gks_last_error(const gks_ctx *ctx);
 int gks_upload(gks_ctx *ctx, int f, double *const W[5]);
 int gks_download(gks_ctx *ctx, int f, double *const W[5]);
 
+/* The reference's per-step call, evolve(W, dev, dt) (GPUupdate.h:33,
+ * GPUupdate.cu:65-196): upload W (padded layout), advance nsteps steps with
+ * the field's dt (gks_set_dt / gks_timestep), download W with its ghosts as
+ * the periodic image.  Synchronous; the state stays resident afterwards.  For
+ * one field and one step the copies overlap the step: W goes up in y-slabs on
+ * one copy stream, each slab's stages run as soon as the planes they read
+ * have arrived, and updated planes come back on another copy stream -- with W
+ * in pinned (page-locked) host memory both PCIe directions and the kernels
+ * run concurrently; pageable W works but overlaps less.  The first such call
+ * allocates 25 nc^3 + 5 (nc+6)^3 doubles of pipeline buffers for the context
+ * (4.1 GB at 256^3).  Otherwise (an ensemble, nsteps > 1, nc < 16) it is
+ * gks_upload + gks_step + gks_download.  Results are bit-identical either way. */
+int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps);
+
 /* Time step: dt = cfl*dx/max(|u|+c) over the interior (timestep,
  * update.cpp:1057-1079); the result is also made the step's dt. */
 int gks_timestep(gks_ctx *ctx, int f, double cfl, double *dt_out);
