@@ -641,6 +641,31 @@ int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps)
     return gks_download(ctx, f, W);
 }
 
+int gks_host_register(void *p, size_t bytes, int *registered)
+{
+    if (registered) *registered = 0;
+    if (!p || bytes == 0) return GKS_EINVAL;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeHost) return GKS_OK;
+    cudaGetLastError(); // an unregistered pointer may leave an error behind on older runtimes
+    if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return GKS_ECUDA;
+    }
+    if (registered) *registered = 1;
+    return GKS_OK;
+}
+
+int gks_host_unregister(void *p)
+{
+    if (!p) return GKS_EINVAL;
+    if (cudaHostUnregister(p) != cudaSuccess) {
+        cudaGetLastError();
+        return GKS_ECUDA;
+    }
+    return GKS_OK;
+}
+
 int gks_set_dt(gks_ctx *ctx, int f, double dt)
 {
     int rc = check_field(ctx, f);

@@ -165,6 +165,29 @@ __device__ __forceinline__ double half_erfc_abs(double x, double ex)
     return (0.5 * ex) * p;
 }
 
+// Both half-space seeds, hp = 0.5 erfc(x) and hm = 0.5 erfc(-x), from x and
+// ex = exp(-x^2).  For |x| <= 1 (nearly every interface of a turbulent field)
+// from erf(x) = x P(x^2), P the generated polynomial of degree kErfSmallDeg in
+// x^2, with no reciprocal: hp = 0.5 - 0.5 x P, hm = 0.5 + 0.5 x P, each one
+// fused multiply-add (relative error below 6.1e-16); beyond, from the erfcx
+// form above, the far tail direct and the other value as 1 - tail.
+__device__ __forceinline__ void half_erfc_pm(double x, double ex, double &hp, double &hm)
+{
+    if (fabs(x) <= 1.0) {
+        const double s = x * x;
+        double p = kErfSmallC[kErfSmallDeg];
+#pragma unroll
+        for (int i = kErfSmallDeg - 1; i >= 0; --i) p = fma(p, s, kErfSmallC[i]);
+        const double hx = 0.5 * x;
+        hp = fma(-hx, p, 0.5);
+        hm = fma(hx, p, 0.5);
+    } else {
+        const double tail = half_erfc_abs(x, ex);
+        hp = x >= 0.0 ? tail : 1.0 - tail;
+        hm = x >= 0.0 ? 1.0 - tail : tail;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // 1-D velocity moments of a Maxwellian (GKMflux.cpp:48-66).  s = 1/(2 lambda)
 // is the variance; <u^n> = U <u^{n-1}> + (n-1) s <u^{n-2}>.

@@ -206,8 +206,8 @@ __device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, 
         const double rl = rsqrt(g.lam), sl = g.lam * rl;
         const double x = NEG ? sl * g.U0 : -sl * g.U0; // h0 = 0.5 erfc(x)
         const double e2 = exp(-g.lam * g.U0 * g.U0);
-        const double tail = half_erfc_abs(x, e2);
-        const double h0 = x >= 0.0 ? tail : 1.0 - tail;
+        double h0, hm;
+        half_erfc_pm(x, e2, h0, hm);
         const double ex = e2 * (kHalfRsqrtPi * rl);
         half_table<7>(g.U0, g.s, h0, NEG ? -ex : ex, Xh);
     }
@@ -470,15 +470,15 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau_n, double ta
     double Xf[6], Xp[7], Xn[7];
     full_table<6, double>(e.U0, e.s, Xf);
     {
-        // 0.5 erfc(-+x) from one evaluation at |x|: the far tail is computed
-        // directly, the other value as 1 - tail (no cancellation)
+        // 0.5 erfc(-+x) from one evaluation (half_erfc_pm)
         const double rl = rsqrt(e.lam), sl = e.lam * rl;
         const double x = sl * e.U0;
         const double e2 = exp(-e.lam * e.U0 * e.U0);
-        const double tail = half_erfc_abs(x, e2);
+        double hp, hm;
+        half_erfc_pm(x, e2, hp, hm);
         const double g = e2 * (kHalfRsqrtPi * rl);
-        half_table<7>(e.U0, e.s, x >= 0.0 ? 1.0 - tail : tail, g, Xp);
-        half_table<7>(e.U0, e.s, x >= 0.0 ? tail : 1.0 - tail, -g, Xn);
+        half_table<7>(e.U0, e.s, hm, g, Xp);
+        half_table<7>(e.U0, e.s, hp, -g, Xn);
     }
     const double c4 = fma(0.5, fma(e.U1, e.U1, e.U2 * e.U2), double(c.K + 2) * 0.5 * e.s);
     // B_ / rho_e in the primed frame of the equilibrium, with its nearly

@@ -715,213 +715,195 @@ __global__ void k_maxwave(FieldDev f, unsigned long long *out)
 // node slopes of the natural cubic spline through each padded grid line
 // (nt = nc + 6 points, periodic ghosts), the interpolant the reference builds
 // with einspline (Interpolation.cpp:3-31); at nodes a tensor-product natural
-// spline reduces to these 1-D slopes.  Scratch layout: [0..2] u, v, w;
-// [3 + 3*comp + axis] d(comp)/d(axis), axis 0 = y, 1 = x, 2 = z.
+// spline reduces to these 1-D slopes.  Scratch layout: [3 + 3*comp + axis]
+// d(comp)/d(axis), axis 0 = y, 1 = x, 2 = z (slots 0-2 unused).
 // ---------------------------------------------------------------------------
-__global__ void k_velocity(FieldDev f, double *scr)
-{
-    const long long n = f.ncell;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
-        const double ri = __drcp_rn(f.W[0][c]);
-        scr[c] = f.W[1][c] * ri;
-        scr[n + c] = f.W[2][c] * ri;
-        scr[2 * n + c] = f.W[3][c] * ri;
-    }
-}
 
-// Slopes of the natural cubic spline through the nt = nc + 6 nodes of every
-// padded periodic grid line along `axis` (the reference's einspline over its
-// padded block), for the three velocity components in turn:
+// Slopes of the natural cubic spline through the nt = nc + 6 nodes of a
+// padded periodic grid line (the reference's einspline over its padded
+// block):
 //   2 m0 + m1 = s (f1 - f0);  m_{p-1} + 4 m_p + m_{p+1} = s (f_{p+1} - f_{p-1});
 //   m_{n-2} + 2 m_{n-1} = s (f_{n-1} - f_{n-2}),  s = 3/h,
-// solved per line by the Thomas algorithm with precomputed pivots: forward
-// d_p = (r_p - d_{p-1}) inv_p, backward m_p = d_p - cp_p m_{p+1}, m_{nt-1} = d_{nt-1}.
-// One warp owns 32 lines, one lane per line.
-constexpr int kSplLines = 32, kSplChunk = 32, kSplPitch = kSplChunk + 3;
+// solved by the Thomas recurrences with precomputed pivots,
+//   forward  d_p = (r_p - d_{p-1}) inv_p,   backward  m_p = d_p - cp_p m_{p+1},
+// each step an affine map of the previous value.  One warp solves one line:
+// lane L owns the SPL_B consecutive nodes [L B, L B + B) (B odd, 32 B >= nt),
+// composes the affine maps of its nodes, an inclusive warp scan of the
+// composed maps (five shuffle steps) hands every lane the value entering its
+// nodes, and the lane runs its nodes again from there -- forward, then the
+// same backward.  The associativity of the scan changes only the rounding.
+// A block stages LW lines of one velocity component in shared memory (the
+// velocity computed from rho and rho u on load, so no separate velocity
+// pass), the warps solve them, and the slopes leave through the same tile:
+//   y, x lines: LW consecutive k of one (i) / (j): tile [node][line], each row
+//               of the tile one coalesced load / store of LW doubles;
+//   z lines:    LW consecutive (j, i) lines:      tile [line][node], each
+//               line one contiguous run of nc doubles.
+// Odd B keeps the solve's shared-memory accesses free of bank conflicts.
+constexpr int kLoadBatch = 9;
 
-// x and y lines (k_spline_stream), one pass per line: the backward recurrence
-// forgets its start by a factor cp_p (-> 2 - sqrt 3 = 0.268) per node, so m_p
-// computed from m = 0 placed kSplTail = 32 nodes above p differs from the
-// exact slope by less than 0.27^32 ~ 5e-19 of the line's largest slope, far
-// below double rounding.  A lane runs the forward recurrence once along its
-// line, keeps the last kSplRing = 64 forward values in its column of a
-// shared-memory ring, and every 32 nodes runs the backward recurrence over
-// the ring, finalising the nodes that have 32 newer ones above them (at the
-// line's end, where m_{nt-1} = d_{nt-1} is exact, all the rest).  Each
-// velocity value is read once and each slope written once; consecutive lanes
-// own neighbouring lines, so every access is a coalesced row.
-constexpr int kSplRing = 64, kSplTail = 32, kSplRingPitch = kSplLines + 1;
-constexpr int kSplStreamWarps = 2; // 2 x 16.9 KB of ring per block
-// z lines (k_spline_tiled) are contiguous along the line, so a lane-per-line
-// access is a 32-way strided one; they take two passes (forward values
-// parked in the slope array, then the exact backward recurrence) through a
-// per-warp tile that turns every global access into a coalesced row.  The
-// streaming form needs ring and tile together, which at this shared-memory
-// footprint per warp halves the resident warps and measured 2.2x slower.
-constexpr int kSplTiledWarps = 4; // 4 x 9 KB of tile per block
-
-__global__ void __launch_bounds__(32 * kSplStreamWarps) k_spline_stream(FieldDev f, double *scr, int axis)
+template <int AXIS, int B, int LW>
+__global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDev f, double *scr)
 {
-    constexpr int NW = kSplStreamWarps;
-    __shared__ double rings[NW][kSplRing][kSplRingPitch];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double (*ring)[kSplRingPitch] = rings[wid];
+    extern __shared__ double smem[];
     const int nc = f.nc, nt = nc + 6;
     const long long n = f.ncell;
-    const long long lines = (long long)nc * nc;
-    const long long line0 = ((long long)blockIdx.x * NW + wid) * kSplLines;
-    if (line0 >= lines) return; // uniform per warp
-    const int nl = int(min((long long)kSplLines, lines - line0));
-    const long long st = axis == 0 ? (long long)nc * nc : (long long)nc;
-    const bool mine = lane < nl;
-    // first cell of this lane's line: (i,k) lines for axis 0, (j,k) for axis 1
-    long long mybase;
-    {
-        const long long L = line0 + (mine ? lane : 0);
-        const long long a = L / nc, b = L - a * nc;
-        mybase = axis == 0 ? a * nc + b : a * nc * nc + b;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double *tile = smem;
+    double *cpv = smem + (AXIS == 2 ? LW * nt : nt * (LW + 1));
+    double *invv = cpv + nt;
+    auto T = [&](int node, int line) -> double & {
+        return AXIS == 2 ? tile[line * nt + node] : tile[node * (LW + 1) + line];
+    };
+    for (int p = threadIdx.x; p < nt; p += blockDim.x) {
+        cpv[p] = f.spl_cp[p];
+        invv[p] = f.spl_inv[p];
     }
+    // the block's lines: y / x lines are (outer, k) with k in [k0, k0 + LW),
+    // outer = i (y lines) or j (x lines); z lines are l in [l0, l0 + LW), l = j nc + i
+    const int nkb = (nc + LW - 1) / LW;
+    const long long set = blockIdx.x;
+    const int outer = AXIS == 2 ? 0 : int(set / nkb);
+    const int k0 = AXIS == 2 ? 0 : int(set - (long long)outer * nkb) * LW;
+    const long long l0 = AXIS == 2 ? set * LW : 0;
+    // cell of line `line` at position q (0 .. nc-1) along the axis
+    auto cell = [&](int line, int q) -> long long {
+        if (AXIS == 0) return ((long long)q * nc + outer) * nc + k0 + line;
+        if (AXIS == 1) return ((long long)outer * nc + q) * nc + k0 + line;
+        return (l0 + line) * nc + q;
+    };
+    auto active = [&](int line) -> bool {
+        return AXIS == 2 ? l0 + line < (long long)nc * nc : k0 + line < nc;
+    };
     const double s = f.spl_s;
-    const double *cp = f.spl_cp, *inv = f.spl_inv;
-    // node p of a line sits at cell wrap(p - 3) along the axis
-    auto node_off = [&](int p) -> long long { return (long long)wrap(p - 3, nc) * st; };
+    const int p0 = lane * B;
+    // the t-th node a thread loads and stores: z, node lane + 32 t of the
+    // warp's line; y, x, row (t LW + w) R + lane / LW of line lane % LW, with
+    // R = 32 / LW rows per warp and step (every lane busy, 32 t covering nt)
+    constexpr int R = 32 / LW;
+    auto node_of = [&](int t) -> int { return AXIS == 2 ? lane + 32 * t : (t * LW + w) * R + lane / LW; };
 
 #pragma unroll 1
     for (int comp = 0; comp < 3; ++comp) {
-        const double *u = scr + comp * n;
-        double *g = scr + (3 + 3 * comp + axis) * n;
-        double dp = 0.0;
-        int fin = 3; // next node to finalise (nodes 0..2 are ghosts)
+        const double *rho = f.W[0], *mom = f.W[1 + comp];
+        double *g = scr + (3 + 3 * comp + AXIS) * n;
+        // stage the line set's velocity: node p holds cell wrap(p - 3); each
+        // thread issues a batch of kLoadBatch loads of rho and rho u before
+        // using any, so that their memory latencies overlap
+        {
+            // z: lane = node of the warp's line; y, x: lane = (row parity, line)
+            constexpr int PER = B;
+            const int line = AXIS == 2 ? w : lane % LW;
+            const bool on = AXIS == 2 ? active(w) : active(lane % LW);
 #pragma unroll 1
-        for (int p0 = 0; p0 < nt; p0 += kSplChunk) {
-            // chunk values v[jj] = node p0 - 1 + jj, jj = 0 .. 33, all loads in flight at once
-            double v[kSplChunk + 2];
+            for (int t0 = 0; t0 < PER; t0 += kLoadBatch) {
+                double vr[kLoadBatch], vm[kLoadBatch];
 #pragma unroll
-            for (int jj = 0; jj < kSplChunk + 2; ++jj) {
-                const int p = p0 - 1 + jj;
-                v[jj] = (mine && p >= 0 && p < nt) ? __ldg(u + mybase + node_off(p)) : 0.0;
-            }
-            // forward recurrence over the chunk's nodes into the ring
-            const int cend = min(kSplChunk, nt - p0);
-#pragma unroll
-            for (int c = 0; c < kSplChunk; ++c) {
-                if (c < cend) {
-                    const int p = p0 + c, jj = c + 1;
-                    if (p == 0) {
-                        dp = (s * (v[jj + 1] - v[jj])) * inv[0];
-                    } else {
-                        const double r = p < nt - 1 ? s * (v[jj + 1] - v[jj - 1]) : s * (v[jj] - v[jj - 1]);
-                        dp = (r - dp) * inv[p];
+                for (int t = 0; t < kLoadBatch; ++t) {
+                    const int p = node_of(t0 + t);
+                    vr[t] = 1.0;
+                    vm[t] = 0.0;
+                    if (on && t0 + t < PER && p < nt) {
+                        const long long c = cell(line, wrap(p - 3, nc));
+                        vr[t] = __ldg(rho + c);
+                        vm[t] = __ldg(mom + c);
                     }
-                    ring[p & (kSplRing - 1)][lane] = dp;
                 }
-            }
-            // finalise: backward from the newest node over the ring; the span
-            // phi - fin stays below kSplRing, so no slot is read after reuse
-            const int phi = p0 + cend - 1;
-            const int last = min(phi == nt - 1 ? phi : phi - kSplTail, nt - 4); // last node to emit
-            if (last >= fin) {
-                double m = 0.0;
-                for (int p = phi; p >= fin; --p) {
-                    double *slot = &ring[p & (kSplRing - 1)][lane];
-                    m = *slot - cp[p] * m;
-                    if (p <= last && mine) g[mybase + (long long)(p - 3) * st] = m;
+#pragma unroll
+                for (int t = 0; t < kLoadBatch; ++t) {
+                    const int p = node_of(t0 + t);
+                    if (on && t0 + t < PER && p < nt) T(p, line) = vm[t] * __drcp_rn(vr[t]);
                 }
-                fin = last + 1;
             }
         }
-    }
-}
-
-__global__ void __launch_bounds__(32 * kSplTiledWarps) k_spline_tiled(FieldDev f, double *scr)
-{
-    constexpr int NW = kSplTiledWarps;
-    __shared__ double tiles[NW][kSplLines][kSplPitch];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double (*tile)[kSplPitch] = tiles[wid];
-    const int nc = f.nc, nt = nc + 6;
-    const long long n = f.ncell;
-    const long long lines = (long long)nc * nc;
-    const long long line0 = ((long long)blockIdx.x * NW + wid) * kSplLines;
-    if (line0 >= lines) return; // uniform per warp
-    const int nl = int(min((long long)kSplLines, lines - line0));
-    const bool mine = lane < nl;
-    // first cell of this lane's (j,i) line; a lane reads another line's base with a shuffle
-    const long long mybase = (line0 + (mine ? lane : 0)) * nc;
-    const double s = f.spl_s;
-    const double *cp = f.spl_cp, *inv = f.spl_inv;
-
-#pragma unroll 1
-    for (int comp = 0; comp < 3; ++comp) {
-        const double *u = scr + comp * n;
-        double *g = scr + (3 + 3 * comp + 2) * n;
-        double dp = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0; // d0..d2: forward values of the last three nodes
-        // forward pass: tile column jj holds node p0 - 1 + jj, jj = 0 .. 33
-#pragma unroll 1
-        for (int p0 = 0; p0 < nt; p0 += kSplChunk) {
+        __syncthreads();
+        if (active(w)) {
+            // right-hand sides of the lane's nodes and the composed forward map d -> A d + C
+            double r[B];
+            double A = 1.0, C = 0.0;
 #pragma unroll
-            for (int l = 0; l < kSplLines; ++l) {
-                const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                const int p = p0 - 1 + lane;
-                if (l < nl && p >= 0 && p < nt) tile[l][lane] = __ldg(u + b + wrap(p - 3, nc));
-                if (lane < 2 && l < nl && p + 32 < nt) tile[l][lane + 32] = __ldg(u + b + wrap(p + 29, nc));
-            }
-            __syncwarp();
-            if (mine) {
-                const int cend = min(kSplChunk, nt - p0);
-                for (int c = 0; c < cend; ++c) {
-                    const int p = p0 + c, jj = c + 1;
-                    if (p == 0) {
-                        dp = (s * (tile[lane][jj + 1] - tile[lane][jj])) * inv[0];
-                    } else {
-                        const double r = p < nt - 1 ? s * (tile[lane][jj + 1] - tile[lane][jj - 1])
-                                                    : s * (tile[lane][jj] - tile[lane][jj - 1]);
-                        dp = (r - dp) * inv[p];
-                    }
-                    if (p == nt - 3) d0 = dp;
-                    else if (p == nt - 2) d1 = dp;
-                    else if (p == nt - 1) d2 = dp;
-                    tile[lane][c] = dp; // column c (node p - 1) is no longer read
+            for (int j = 0; j < B; ++j) {
+                const int p = p0 + j;
+                if (p < nt) {
+                    // rows 0 and nt-1 are the one-sided natural-end rows
+                    const double fa = p == 0 ? T(0, w) : T(p - 1, w);
+                    const double fb = p == nt - 1 ? T(p, w) : T(p + 1, w);
+                    r[j] = s * (fb - fa);
+                    const double iv = invv[p];
+                    A = -iv * A;
+                    C = (r[j] - C) * iv;
                 }
             }
-            __syncwarp();
-            // park forward values of nodes 3 .. nt-4 at cell p - 3
-            const int p = p0 + lane;
 #pragma unroll
-            for (int l = 0; l < kSplLines; ++l) {
-                const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                if (l < nl && p >= 3 && p <= nt - 4) g[b + (long long)(p - 3)] = tile[l][lane];
+            for (int off = 1; off < 32; off <<= 1) {
+                const double Ap = __shfl_up_sync(0xffffffffu, A, off);
+                const double Cp = __shfl_up_sync(0xffffffffu, C, off);
+                if (lane >= off) {
+                    C = A * Cp + C;
+                    A = A * Ap;
+                }
             }
-            __syncwarp();
-        }
-        // backward pass over cells q = p - 3 = nc-1 .. 0, in chunks from the top
-        double m = d2;
-        m = d1 - cp[nt - 2] * m;
-        m = d0 - cp[nt - 3] * m;
-#pragma unroll 1
-        for (int q0 = ((nc - 1) / kSplChunk) * kSplChunk; q0 >= 0; q0 -= kSplChunk) {
-            const int cnt = min(kSplChunk, nc - q0);
+            double d = __shfl_up_sync(0xffffffffu, C, 1);
+            if (lane == 0) d = 0.0;
 #pragma unroll
-            for (int l = 0; l < kSplLines; ++l) {
-                const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                if (l < nl && lane < cnt) tile[l][lane] = g[b + (long long)(q0 + lane)];
+            for (int j = 0; j < B; ++j) {
+                const int p = p0 + j;
+                if (p < nt) {
+                    d = (r[j] - d) * invv[p];
+                    r[j] = d;
+                }
             }
-            __syncwarp();
-            if (mine) {
-                for (int c = cnt - 1; c >= 0; --c) {
-                    m = tile[lane][c] - cp[q0 + c + 3] * m;
-                    tile[lane][c] = m;
+            // backward: the composed map m_next -> G m_next + H of the lane's nodes
+            double G = 1.0, H = 0.0;
+#pragma unroll
+            for (int j = B - 1; j >= 0; --j) {
+                const int p = p0 + j;
+                if (p < nt) {
+                    const double c = cpv[p];
+                    H = r[j] - c * H;
+                    G = -c * G;
+                }
+            }
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const double Gn = __shfl_down_sync(0xffffffffu, G, off);
+                const double Hn = __shfl_down_sync(0xffffffffu, H, off);
+                if (lane + off < 32) {
+                    H = G * Hn + H;
+                    G = G * Gn;
+                }
+            }
+            double m = __shfl_down_sync(0xffffffffu, H, 1);
+            if (lane == 31) m = 0.0;
+#pragma unroll
+            for (int j = B - 1; j >= 0; --j) {
+                const int p = p0 + j;
+                if (p < nt) {
+                    m = r[j] - cpv[p] * m;
+                    r[j] = m;
                 }
             }
             __syncwarp();
 #pragma unroll
-            for (int l = 0; l < kSplLines; ++l) {
-                const long long b = __shfl_sync(0xffffffffu, mybase, l);
-                if (l < nl && lane < cnt) g[b + (long long)(q0 + lane)] = tile[l][lane];
+            for (int j = 0; j < B; ++j) {
+                const int p = p0 + j;
+                if (p < nt) T(p, w) = r[j];
             }
-            __syncwarp();
         }
+        __syncthreads();
+        // slopes of nodes 3 .. nt-4 (cells 0 .. nc-1)
+        {
+            const int line = AXIS == 2 ? w : lane % LW;
+            const bool on = AXIS == 2 ? active(w) : active(lane % LW);
+            if (on) {
+#pragma unroll 4
+                for (int t = 0; t < B; ++t) {
+                    const int p = node_of(t);
+                    if (p >= 3 && p <= nt - 4) g[cell(line, p - 3)] = T(p, line);
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -1202,16 +1184,40 @@ cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int 
     return cudaGetLastError();
 }
 
+template <int AXIS, int B, int LW>
+cudaError_t spline_go(const FieldDev &f, double *scratch, cudaStream_t st)
+{
+    const int nt = f.nc + 6;
+    const size_t bytes = ((AXIS == 2 ? (size_t)LW * nt : (size_t)nt * (LW + 1)) + 2 * (size_t)nt) * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_spline_scan<AXIS, B, LW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes);
+    if (e != cudaSuccess) return e;
+    const long long sets = AXIS == 2 ? ((long long)f.nc * f.nc + LW - 1) / LW
+                                     : (long long)f.nc * ((f.nc + LW - 1) / LW);
+    k_spline_scan<AXIS, B, LW><<<(unsigned)sets, 32 * LW, bytes, st>>>(f, scratch);
+    return cudaGetLastError();
+}
+
+// Nodes per lane B (odd, 32 B >= nt) and lines per block LW = 16 (the tile of
+// one component within 160 KB of shared memory; two blocks per SM up to B = 9).
+template <int AXIS>
+cudaError_t spline_axis(const FieldDev &f, double *scratch, cudaStream_t st)
+{
+    const int nt = f.nc + 6;
+    if (nt <= 160) return spline_go<AXIS, 5, 16>(f, scratch, st);
+    if (nt <= 288) return spline_go<AXIS, 9, 16>(f, scratch, st);
+    if (nt <= 544) return spline_go<AXIS, 17, 16>(f, scratch, st);
+    return spline_go<AXIS, 33, 16>(f, scratch, st);
+}
+
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st)
 {
     const int block = 256;
     const int grid = stats_grid(f.ncell, block, nsm); // partial holds stats_partial_elems(nsm) >= kStatsSums * grid
-    k_velocity<<<grid, block, 0, st>>>(f, scratch);
-    const long long lines = (long long)f.nc * f.nc;
-    auto lgrid = [&](int nw) { return int((lines + kSplLines * nw - 1) / (kSplLines * nw)); };
-    for (int axis = 0; axis < 2; ++axis)
-        k_spline_stream<<<lgrid(kSplStreamWarps), 32 * kSplStreamWarps, 0, st>>>(f, scratch, axis);
-    k_spline_tiled<<<lgrid(kSplTiledWarps), 32 * kSplTiledWarps, 0, st>>>(f, scratch);
+    cudaError_t e = spline_axis<0>(f, scratch, st);
+    if (e == cudaSuccess) e = spline_axis<1>(f, scratch, st);
+    if (e == cudaSuccess) e = spline_axis<2>(f, scratch, st);
+    if (e != cudaSuccess) return e;
     k_sums1<<<grid, block, 0, st>>>(f, scratch, partial);
     k_finalize<<<1, 32 * NSUM1, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
     return cudaGetLastError();

@@ -119,7 +119,8 @@ cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream
 // *out_bits must be zero on entry).
 cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int nsm, cudaStream_t st);
 
-// Statistics of one field.  scratch: 12 * nc^3 doubles; partial: stats_partial_elems(nsm) doubles.
+// Statistics of one field.  scratch: 12 * nc^3 doubles (the first 3 unused); partial:
+// stats_partial_elems(nsm) doubles.
 // Writes 24 means into sums[0..23]: the 18 PrintStats means and, for p, T and
 // 1/rho, the means of x - K and (x - K)^2 (K = the value at cell 0).
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st);

@@ -15,6 +15,11 @@
 //   GKS_COMPAT_GPU_SEMANTICS  reproduce the reference GPU kernel's choices
 //                             (WENO on rho E, no 1/Pr factor) instead of the
 //                             CPU path's (the parity default)
+//   GKS_COMPAT_NO_PIN         leave the caller's W arrays pageable (by default
+//                             the first evolve() page-locks them with
+//                             cudaHostRegister, as the overlapped copies need,
+//                             and ~DevAlloc releases them; the reference
+//                             allocates W once per run, Main.cpp:36)
 // As in the reference, evolve() uploads W, advances one step and downloads W
 // (gks_evolve: the copies overlap the step slab by slab; with W in pinned host
 // memory both PCIe directions and the step run concurrently); the downloaded
@@ -33,10 +38,45 @@ class DevAlloc
 {
 public:
     DevAlloc();
-    ~DevAlloc() { gks_destroy(ctx); }
+    ~DevAlloc()
+    {
+        unpin();
+        gks_destroy(ctx);
+    }
     DevAlloc(const DevAlloc &) = delete;
     DevAlloc &operator=(const DevAlloc &) = delete;
     gks_ctx *ctx = nullptr;
+    // the host arrays page-locked by pin() (null: none)
+    void *pinned[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t pinned_bytes = 0;
+
+    // Page-lock the five arrays of W (nt^3 doubles each) unless they already
+    // are; a different W than last time replaces the earlier registration.
+    void pin(ptype *W[5])
+    {
+#ifndef GKS_COMPAT_NO_PIN
+        const size_t bytes = (size_t)Nt_seg * sizeof(ptype);
+        bool same = bytes == pinned_bytes;
+        for (int q = 0; q < 5 && same; ++q) same = pinned[q] == (void *)W[q];
+        if (same) return;
+        unpin();
+        for (int q = 0; q < 5; ++q) {
+            int made = 0;
+            // a failure leaves W pageable: the copies still work, overlapping less
+            if (gks_host_register(W[q], bytes, &made) == GKS_OK && made) pinned[q] = W[q];
+        }
+        pinned_bytes = bytes;
+#else
+        (void)W;
+#endif
+    }
+    void unpin()
+    {
+        for (int q = 0; q < 5; ++q)
+            if (pinned[q]) gks_host_unregister(pinned[q]);
+        for (int q = 0; q < 5; ++q) pinned[q] = nullptr;
+        pinned_bytes = 0;
+    }
 };
 
 inline void gks_compat_check(gks_ctx *ctx, int rc, const char *what)
@@ -82,6 +122,7 @@ inline DevAlloc::DevAlloc()
 
 inline void evolve(ptype *W[5], DevAlloc *dev, ptype dt)
 {
+    dev->pin(W);
     gks_compat_check(dev->ctx, gks_set_dt(dev->ctx, 0, dt), "gks_set_dt");
     gks_compat_check(dev->ctx, gks_evolve(dev->ctx, 0, W, 1), "gks_evolve");
     gks_compat_check(dev->ctx, gks_sync(dev->ctx), "gks_sync");

@@ -75,6 +75,8 @@ SIGNATURES = {
     "gks_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
     "gks_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5]),
     "gks_evolve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP5, ctypes.c_int]),
+    "gks_host_register": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int)]),
+    "gks_host_unregister": (ctypes.c_int, [ctypes.c_void_p]),
     "gks_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, DP]),
     "gks_set_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]),
     "gks_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

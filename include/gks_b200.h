@@ -31,6 +31,8 @@
 #ifndef GKS_B200_H
 #define GKS_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -118,6 +120,15 @@ int gks_download(gks_ctx *ctx, int f, double *const W[5]);
  * (4.1 GB at 256^3).  Otherwise (an ensemble, nsteps > 1, nc < 16) it is
  * gks_upload + gks_step + gks_download.  Results are bit-identical either way. */
 int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps);
+
+/* Page-lock `bytes` of caller memory at p (cudaHostRegister) so that copies
+ * from and to it run asynchronously at full PCIe rate -- what gks_evolve
+ * needs to overlap them.  *registered (may be NULL) is set to 1 if this call
+ * registered the range, 0 if it was page-locked already (nothing done).
+ * Release with gks_host_unregister before freeing the memory.  No counterpart
+ * in the reference, which copies from pageable memory (GPUupdate.cu:74-78). */
+int gks_host_register(void *p, size_t bytes, int *registered);
+int gks_host_unregister(void *p);
 
 /* Time step: dt = cfl*dx/max(|u|+c) over the interior (timestep,
  * update.cpp:1057-1079); the result is also made the step's dt. */

@@ -9,7 +9,7 @@
 
 typedef double ptype;  // param.h:22
 #define R 287.0        // param.h:18
-int nc_segx, nc_segy, nc_segz, K, procDim[3];
+int nc_segx, nc_segy, nc_segz, K, procDim[3], Nt_seg;
 ptype T0, mu0, den0, p0, Mt, gam, t0;
 
 #include "gks_compat.h"
@@ -31,6 +31,7 @@ int main(int argc, char **argv)
     K = int((5.0 - 3.0 * gam) / (gam - 1.0)); // FlowField.cpp:41
     T0 = p0 / (R * den0);                     // FlowField.cpp:46
     const size_t nt = nc + 6, N = nt * nt * nt;
+    Nt_seg = (int)N; // FlowField.cpp:29
     std::vector<double> buf(5 * N);
     FILE *f = fopen(argv[1], "rb");
     if (!f || fread(buf.data(), sizeof(double), 5 * N, f) != 5 * N) return 3;

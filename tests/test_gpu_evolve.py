@@ -95,3 +95,33 @@ def test_evolve_fallbacks_and_errors(gks):
         with pytest.raises(gks.GksError) as ei:
             s.evolve(Ws[1].copy())
         assert ei.value.code == -4
+
+
+def test_host_register_pins_a_pageable_field(gks):
+    """gks_host_register page-locks caller memory (reporting whether it did),
+    leaves already pinned memory alone, and evolve gives the same answer on
+    the registered array."""
+    import ctypes
+
+    lib = gks.load_library()
+    nc = 24
+    case = gks_ic.make_dhit(nc, k0=4.0, Mt=0.4, seed=7)
+    W0 = gks_ic.to_conservative_padded(case)
+    W = W0.copy()
+    made = ctypes.c_int(-1)
+    ptrs = [W[q].ctypes.data for q in range(5)]
+    for p in ptrs:
+        assert lib.gks_host_register(ctypes.c_void_p(p), W[0].nbytes, ctypes.byref(made)) == 0
+        assert made.value == 1
+    assert lib.gks_host_register(ctypes.c_void_p(ptrs[0]), W[0].nbytes, ctypes.byref(made)) == 0
+    assert made.value == 0  # already page-locked: nothing done
+    try:
+        with gks.Solver(gks.phys_from_case(case)) as s:
+            s.upload(W0)
+            dt = s.timestep(0.5)
+            s.evolve(W)
+        assert np.array_equal(W, plain(gks, case, W0, gks.FP64, dt))
+    finally:
+        for p in ptrs:
+            assert lib.gks_host_unregister(ctypes.c_void_p(p)) == 0
+    assert lib.gks_host_register(None, 8, None) == -1
