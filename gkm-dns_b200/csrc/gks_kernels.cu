@@ -727,33 +727,42 @@ __global__ void k_maxwave(FieldDev f, unsigned long long *out)
 // solved by the Thomas recurrences with precomputed pivots,
 //   forward  d_p = (r_p - d_{p-1}) inv_p,   backward  m_p = d_p - cp_p m_{p+1},
 // each step an affine map of the previous value.  One warp solves one line:
-// lane L owns the SPL_B consecutive nodes [L B, L B + B) (B odd, 32 B >= nt),
+// lane L owns the B consecutive nodes [L B, L B + B) (B odd, 32 B >= nt),
 // composes the affine maps of its nodes, an inclusive warp scan of the
 // composed maps (five shuffle steps) hands every lane the value entering its
 // nodes, and the lane runs its nodes again from there -- forward, then the
 // same backward.  The associativity of the scan changes only the rounding.
-// A block stages LW lines of one velocity component in shared memory (the
-// velocity computed from rho and rho u on load, so no separate velocity
-// pass), the warps solve them, and the slopes leave through the same tile:
-//   y, x lines: LW consecutive k of one (i) / (j): tile [node][line], each row
-//               of the tile one coalesced load / store of LW doubles;
-//   z lines:    LW consecutive (j, i) lines:      tile [line][node], each
+//
+// A block takes LW lines: it copies rho, rho u, rho v, rho w of all their
+// nodes into shared memory with asynchronous copies (all in flight at once,
+// no registers), turns the momenta into velocities in place, each warp solves
+// its line for the components (NCI of them interleaved, for latency), and the
+// slopes leave through the same tiles:
+//   y, x lines: LW consecutive k of one (i) / (j): tiles [node][line], every
+//               group of LW threads one contiguous run of LW doubles;
+//   z lines:    LW consecutive (j, i) lines:      tiles [line][node], each
 //               line one contiguous run of nc doubles.
 // Odd B keeps the solve's shared-memory accesses free of bank conflicts.
-constexpr int kLoadBatch = 9;
+template <int AXIS, int B, int LW> struct SplineTiles {
+    static constexpr int NCI = B <= 9 ? 3 : 1; // components solved together
+    __host__ __device__ static int tile(int nt) { return AXIS == 2 ? LW * nt : nt * (LW + 1); }
+    __host__ __device__ static size_t bytes(int nt) { return (4 * (size_t)tile(nt) + 2 * (size_t)nt) * sizeof(double); }
+};
 
 template <int AXIS, int B, int LW>
 __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDev f, double *scr)
 {
+    using ST = SplineTiles<AXIS, B, LW>;
+    constexpr int NCI = ST::NCI;
     extern __shared__ double smem[];
     const int nc = f.nc, nt = nc + 6;
     const long long n = f.ncell;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double *tile = smem;
-    double *cpv = smem + (AXIS == 2 ? LW * nt : nt * (LW + 1));
-    double *invv = cpv + nt;
-    auto T = [&](int node, int line) -> double & {
-        return AXIS == 2 ? tile[line * nt + node] : tile[node * (LW + 1) + line];
+    const int tsz = ST::tile(nt);
+    double *cpv = smem + 4 * tsz, *invv = cpv + nt;
+    // tile a (0 rho, 1-3 the velocity components), node, line
+    auto T = [&](int a, int node, int line) -> double & {
+        return AXIS == 2 ? smem[a * tsz + line * nt + node] : smem[a * tsz + node * (LW + 1) + line];
     };
     for (int p = threadIdx.x; p < nt; p += blockDim.x) {
         cpv[p] = f.spl_cp[p];
@@ -775,136 +784,161 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
     auto active = [&](int line) -> bool {
         return AXIS == 2 ? l0 + line < (long long)nc * nc : k0 + line < nc;
     };
-    const double s = f.spl_s;
-    const int p0 = lane * B;
-    // the t-th node a thread loads and stores: z, node lane + 32 t of the
-    // warp's line; y, x, row (t LW + w) R + lane / LW of line lane % LW, with
-    // R = 32 / LW rows per warp and step (every lane busy, 32 t covering nt)
-    constexpr int R = 32 / LW;
-    auto node_of = [&](int t) -> int { return AXIS == 2 ? lane + 32 * t : (t * LW + w) * R + lane / LW; };
-
-#pragma unroll 1
-    for (int comp = 0; comp < 3; ++comp) {
-        const double *rho = f.W[0], *mom = f.W[1 + comp];
-        double *g = scr + (3 + 3 * comp + AXIS) * n;
-        // stage the line set's velocity: node p holds cell wrap(p - 3); each
-        // thread issues a batch of kLoadBatch loads of rho and rho u before
-        // using any, so that their memory latencies overlap
-        {
-            // z: lane = node of the warp's line; y, x: lane = (row parity, line)
-            constexpr int PER = B;
-            const int line = AXIS == 2 ? w : lane % LW;
-            const bool on = AXIS == 2 ? active(w) : active(lane % LW);
-#pragma unroll 1
-            for (int t0 = 0; t0 < PER; t0 += kLoadBatch) {
-                double vr[kLoadBatch], vm[kLoadBatch];
-#pragma unroll
-                for (int t = 0; t < kLoadBatch; ++t) {
-                    const int p = node_of(t0 + t);
-                    vr[t] = 1.0;
-                    vm[t] = 0.0;
-                    if (on && t0 + t < PER && p < nt) {
-                        const long long c = cell(line, wrap(p - 3, nc));
-                        vr[t] = __ldg(rho + c);
-                        vm[t] = __ldg(mom + c);
-                    }
-                }
-#pragma unroll
-                for (int t = 0; t < kLoadBatch; ++t) {
-                    const int p = node_of(t0 + t);
-                    if (on && t0 + t < PER && p < nt) T(p, line) = vm[t] * __drcp_rn(vr[t]);
-                }
+    // visit every (node, line) of the set: y / x, LW consecutive threads on
+    // the LW lines of one node; z, warp w along the nodes of line w
+    auto each = [&](auto fn) {
+        if (AXIS == 2) {
+            if (active(w))
+                for (int p = lane; p < nt; p += 32) fn(p, w);
+        } else {
+            for (int e = threadIdx.x; e < nt * LW; e += 32 * LW) {
+                const int line = e % LW;
+                if (active(line)) fn(e / LW, line);
             }
         }
-        __syncthreads();
-        if (active(w)) {
-            // right-hand sides of the lane's nodes and the composed forward map d -> A d + C
-            double r[B];
-            double A = 1.0, C = 0.0;
+    };
+    // stage rho and the momenta (node p holds cell wrap(p - 3)), then velocities
+    each([&](int p, int line) {
+        const long long c = cell(line, wrap(p - 3, nc));
+#pragma unroll
+        for (int a = 0; a < 4; ++a) cp_async8(&T(a, p, line), f.W[a] + c);
+    });
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    each([&](int p, int line) {
+        const double ri = __drcp_rn(T(0, p, line));
+#pragma unroll
+        for (int a = 1; a < 4; ++a) T(a, p, line) *= ri;
+    });
+    __syncthreads();
+    if (active(w)) {
+        const double s = f.spl_s;
+        const int p0 = lane * B;
+#pragma unroll 1
+        for (int c0 = 0; c0 < 3; c0 += NCI) {
+            // right-hand sides and the composed forward maps d -> A d + C of the lane's nodes
+            double r[NCI][B], A[NCI], C[NCI];
+#pragma unroll
+            for (int q = 0; q < NCI; ++q) {
+                A[q] = 1.0;
+                C[q] = 0.0;
+            }
 #pragma unroll
             for (int j = 0; j < B; ++j) {
                 const int p = p0 + j;
                 if (p < nt) {
-                    // rows 0 and nt-1 are the one-sided natural-end rows
-                    const double fa = p == 0 ? T(0, w) : T(p - 1, w);
-                    const double fb = p == nt - 1 ? T(p, w) : T(p + 1, w);
-                    r[j] = s * (fb - fa);
                     const double iv = invv[p];
-                    A = -iv * A;
-                    C = (r[j] - C) * iv;
+                    // rows 0 and nt-1 are the one-sided natural-end rows
+                    const int pa = p == 0 ? 0 : p - 1, pb = p == nt - 1 ? p : p + 1;
+#pragma unroll
+                    for (int q = 0; q < NCI; ++q) {
+                        r[q][j] = s * (T(1 + c0 + q, pb, w) - T(1 + c0 + q, pa, w));
+                        A[q] = -iv * A[q];
+                        C[q] = (r[q][j] - C[q]) * iv;
+                    }
                 }
             }
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
-                const double Ap = __shfl_up_sync(0xffffffffu, A, off);
-                const double Cp = __shfl_up_sync(0xffffffffu, C, off);
-                if (lane >= off) {
-                    C = A * Cp + C;
-                    A = A * Ap;
+#pragma unroll
+                for (int q = 0; q < NCI; ++q) {
+                    const double Ap = __shfl_up_sync(0xffffffffu, A[q], off);
+                    const double Cp = __shfl_up_sync(0xffffffffu, C[q], off);
+                    if (lane >= off) {
+                        C[q] = A[q] * Cp + C[q];
+                        A[q] = A[q] * Ap;
+                    }
                 }
             }
-            double d = __shfl_up_sync(0xffffffffu, C, 1);
-            if (lane == 0) d = 0.0;
+            double d[NCI];
+#pragma unroll
+            for (int q = 0; q < NCI; ++q) {
+                d[q] = __shfl_up_sync(0xffffffffu, C[q], 1);
+                if (lane == 0) d[q] = 0.0;
+            }
 #pragma unroll
             for (int j = 0; j < B; ++j) {
                 const int p = p0 + j;
                 if (p < nt) {
-                    d = (r[j] - d) * invv[p];
-                    r[j] = d;
+                    const double iv = invv[p];
+#pragma unroll
+                    for (int q = 0; q < NCI; ++q) {
+                        d[q] = (r[q][j] - d[q]) * iv;
+                        r[q][j] = d[q];
+                    }
                 }
             }
-            // backward: the composed map m_next -> G m_next + H of the lane's nodes
-            double G = 1.0, H = 0.0;
+            // backward: the composed maps m_next -> G m_next + H of the lane's nodes
+            double G[NCI], H[NCI];
+#pragma unroll
+            for (int q = 0; q < NCI; ++q) {
+                G[q] = 1.0;
+                H[q] = 0.0;
+            }
 #pragma unroll
             for (int j = B - 1; j >= 0; --j) {
                 const int p = p0 + j;
                 if (p < nt) {
-                    const double c = cpv[p];
-                    H = r[j] - c * H;
-                    G = -c * G;
+                    const double cc = cpv[p];
+#pragma unroll
+                    for (int q = 0; q < NCI; ++q) {
+                        H[q] = r[q][j] - cc * H[q];
+                        G[q] = -cc * G[q];
+                    }
                 }
             }
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
-                const double Gn = __shfl_down_sync(0xffffffffu, G, off);
-                const double Hn = __shfl_down_sync(0xffffffffu, H, off);
-                if (lane + off < 32) {
-                    H = G * Hn + H;
-                    G = G * Gn;
+#pragma unroll
+                for (int q = 0; q < NCI; ++q) {
+                    const double Gn = __shfl_down_sync(0xffffffffu, G[q], off);
+                    const double Hn = __shfl_down_sync(0xffffffffu, H[q], off);
+                    if (lane + off < 32) {
+                        H[q] = G[q] * Hn + H[q];
+                        G[q] = G[q] * Gn;
+                    }
                 }
             }
-            double m = __shfl_down_sync(0xffffffffu, H, 1);
-            if (lane == 31) m = 0.0;
+            double m[NCI];
+#pragma unroll
+            for (int q = 0; q < NCI; ++q) {
+                m[q] = __shfl_down_sync(0xffffffffu, H[q], 1);
+                if (lane == 31) m[q] = 0.0;
+            }
 #pragma unroll
             for (int j = B - 1; j >= 0; --j) {
                 const int p = p0 + j;
                 if (p < nt) {
-                    m = r[j] - cpv[p] * m;
-                    r[j] = m;
+                    const double cc = cpv[p];
+#pragma unroll
+                    for (int q = 0; q < NCI; ++q) {
+                        m[q] = r[q][j] - cc * m[q];
+                        r[q][j] = m[q];
+                    }
+                }
+            }
+            __syncwarp(); // every lane has read its neighbours' velocities
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                const int p = p0 + j;
+                if (p < nt) {
+#pragma unroll
+                    for (int q = 0; q < NCI; ++q) T(1 + c0 + q, p, w) = r[q][j];
                 }
             }
             __syncwarp();
-#pragma unroll
-            for (int j = 0; j < B; ++j) {
-                const int p = p0 + j;
-                if (p < nt) T(p, w) = r[j];
-            }
         }
-        __syncthreads();
-        // slopes of nodes 3 .. nt-4 (cells 0 .. nc-1)
-        {
-            const int line = AXIS == 2 ? w : lane % LW;
-            const bool on = AXIS == 2 ? active(w) : active(lane % LW);
-            if (on) {
-#pragma unroll 4
-                for (int t = 0; t < B; ++t) {
-                    const int p = node_of(t);
-                    if (p >= 3 && p <= nt - 4) g[cell(line, p - 3)] = T(p, line);
-                }
-            }
-        }
-        __syncthreads();
     }
+    __syncthreads();
+    // slopes of nodes 3 .. nt-4 (cells 0 .. nc-1)
+    each([&](int p, int line) {
+        if (p >= 3 && p <= nt - 4) {
+            const long long c = cell(line, p - 3);
+#pragma unroll
+            for (int a = 1; a < 4; ++a) scr[(3 + 3 * (a - 1) + AXIS) * n + c] = T(a, p, line);
+        }
+    });
 }
 
 constexpr int NSUM1 = kStatsSums;
@@ -1187,8 +1221,7 @@ cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int 
 template <int AXIS, int B, int LW>
 cudaError_t spline_go(const FieldDev &f, double *scratch, cudaStream_t st)
 {
-    const int nt = f.nc + 6;
-    const size_t bytes = ((AXIS == 2 ? (size_t)LW * nt : (size_t)nt * (LW + 1)) + 2 * (size_t)nt) * sizeof(double);
+    const size_t bytes = SplineTiles<AXIS, B, LW>::bytes(f.nc + 6);
     cudaError_t e = cudaFuncSetAttribute(k_spline_scan<AXIS, B, LW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)bytes);
     if (e != cudaSuccess) return e;
@@ -1198,16 +1231,17 @@ cudaError_t spline_go(const FieldDev &f, double *scratch, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Nodes per lane B (odd, 32 B >= nt) and lines per block LW = 16 (the tile of
-// one component within 160 KB of shared memory; two blocks per SM up to B = 9).
+// Nodes per lane B (odd, 32 B >= nt) and lines per block LW: 8 lines (64
+// contiguous bytes per row of a y / x tile) up to nt = 288, 4 beyond, so that
+// the four tiles stay within 170 KB of shared memory.
 template <int AXIS>
 cudaError_t spline_axis(const FieldDev &f, double *scratch, cudaStream_t st)
 {
     const int nt = f.nc + 6;
-    if (nt <= 160) return spline_go<AXIS, 5, 16>(f, scratch, st);
-    if (nt <= 288) return spline_go<AXIS, 9, 16>(f, scratch, st);
-    if (nt <= 544) return spline_go<AXIS, 17, 16>(f, scratch, st);
-    return spline_go<AXIS, 33, 16>(f, scratch, st);
+    if (nt <= 160) return spline_go<AXIS, 5, 8>(f, scratch, st);
+    if (nt <= 288) return spline_go<AXIS, 9, 8>(f, scratch, st);
+    if (nt <= 544) return spline_go<AXIS, 17, 4>(f, scratch, st);
+    return spline_go<AXIS, 33, 4>(f, scratch, st);
 }
 
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st)
