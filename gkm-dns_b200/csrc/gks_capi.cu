@@ -134,10 +134,18 @@ int ensure_stage(gks_ctx *ctx, int f)
     return GKS_OK;
 }
 
+// Publish field f's descriptor: to the device array every kernel of an
+// ensemble reads, and for a one-field context also into the launch
+// parameters (Batch::one), which a captured step graph holds by value, so
+// the graph is captured again on the next step.
 int push_field(gks_ctx *ctx, int f)
 {
     CK(cudaMemcpyAsync(ctx->d_fields + f, &ctx->fh[f].dev, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->nfields == 1) {
+        ctx->batch.one = ctx->fh[0].dev;
+        drop_graph(ctx);
+    }
     return GKS_OK;
 }
 
@@ -292,6 +300,7 @@ int pipe_stage(gks_ctx *ctx, const FieldDev &d, int kind, int dir, long long p0,
     if (p1 <= p0) return GKS_OK;
     const long long nc = d.nc;
     gks::Batch b = ctx->batch;
+    b.one = d; // this step's descriptor (spare state, per-sweep reconstruction buffers)
     gks::LaunchCfg c = ctx->cfg[kind][dir];
     long long per_plane = nc * nc; // cells
     if (kind == gks::K_RECON && c.variant < 3) {
@@ -425,6 +434,8 @@ int evolve_pipelined(gks_ctx *ctx, double *const W[5])
     }
     CK(cudaMemcpyAsync(ctx->d_fields, &h.dev, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->batch.one = h.dev;
+    drop_graph(ctx);
     h.uploaded = true;
     return GKS_OK;
 }
@@ -555,6 +566,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     ctx->batch.wtotal = wbase;
     ctx->batch.ztotal = zbase;
     ctx->batch.err = ctx->d_err;
+    ctx->batch.one = ctx->fh[0].dev;
     choose_launch(ctx);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(GKS_ECUDA);
     *out = ctx;

@@ -40,31 +40,40 @@ namespace gks {
 
 constexpr double kHalfRsqrtPi = 0.28209479177387814; // 1 / (2 sqrt(pi))
 
-// Constants of one Maxwellian in its transverse co-moving frame.  The
-// negated copies let every use be a plain fused multiply-add, also for the
-// paired type f2, whose instructions take no operand negation.
+// Constants of one Maxwellian in its transverse co-moving frame.  The paired
+// type f2 takes no operand negation, so for it the negatives are kept as
+// well, making every use a plain fused multiply-add; in double a negated
+// operand is free, and the negatives are formed at the use.
 template <typename T> struct CoFrame {
-    T U1, U2, hu2;        // transverse velocity, hu2 = (U1^2 + U2^2)/2 (to_lab)
-    T nU1, nU2, nhu2;     // their negatives (to_prime)
-    T nU0, m2U0, nqn, nqh; // -U0, -2 U0, -qn, -qn/2 with qn = U0^2 + (K+3) s (solve)
-    T tl, kal2;           // 2 lambda, kA lambda^2 (solve)
-    T s, r2, r4, q4;      // 1/(2 lambda), <rho^2>, <rho^4>, <c1^2 rho^2> (moments)
+    T U0, U1, U2, hu2;     // normal and transverse velocity, hu2 = (U1^2 + U2^2)/2 (to_lab)
+    T nU0_, nU1_, nU2_, nhu2_; // their negatives (f2 only)
+    T m2U0, nqn, nqh;      // -2 U0, -qn, -qn/2 with qn = U0^2 + (K+3) s (solve)
+    T tl, kal2;            // 2 lambda, kA lambda^2 (solve)
+    T s, r2, r4, q4;       // 1/(2 lambda), <rho^2>, <rho^4>, <c1^2 rho^2> (moments)
+    static constexpr bool kDouble = std::is_same<T, double>::value;
+    __device__ __forceinline__ T nU0() const { if constexpr (kDouble) return -U0; else return nU0_; }
+    __device__ __forceinline__ T nU1() const { if constexpr (kDouble) return -U1; else return nU1_; }
+    __device__ __forceinline__ T nU2() const { if constexpr (kDouble) return -U2; else return nU2_; }
+    __device__ __forceinline__ T nhu2() const { if constexpr (kDouble) return -hu2; else return nhu2_; }
 };
 
 template <typename T>
 __device__ __forceinline__ CoFrame<T> co_frame(T U0, T U1, T U2, T s, T lam, int K, T kA)
 {
     CoFrame<T> f;
+    f.U0 = U0;
     f.U1 = U1;
     f.U2 = U2;
     f.hu2 = T(0.5f) * fmaT(U1, U1, U2 * U2);
     const T m1 = T(-1.0f);
-    f.nU1 = m1 * U1;
-    f.nU2 = m1 * U2;
-    f.nhu2 = m1 * f.hu2;
-    f.nU0 = m1 * U0;
+    if constexpr (!CoFrame<T>::kDouble) {
+        f.nU0_ = m1 * U0;
+        f.nU1_ = m1 * U1;
+        f.nU2_ = m1 * U2;
+        f.nhu2_ = m1 * f.hu2;
+    }
     f.m2U0 = T(-2.0f) * U0;
-    f.nqn = fmaT(f.nU0, U0, T(float(-(K + 3))) * s);
+    f.nqn = fmaT(f.nU0(), U0, T(float(-(K + 3))) * s);
     f.nqh = T(0.5f) * f.nqn;
     f.tl = T(2.0f) * lam;
     f.kal2 = (kA * lam) * lam;
@@ -97,7 +106,7 @@ __device__ __forceinline__ void to_prime(T b[5], T nU1, T nU2, T nhu2)
 template <typename T>
 __device__ __forceinline__ void to_prime(T b[5], const CoFrame<T> &f)
 {
-    to_prime<T>(b, f.nU1, f.nU2, f.nhu2);
+    to_prime<T>(b, f.nU1(), f.nU2(), f.nhu2());
 }
 
 // Slope solve (slopesolver, GKMflux.cpp:280-296) in the primed frame: the
@@ -107,13 +116,13 @@ __device__ __forceinline__ void to_prime(T b[5], const CoFrame<T> &f)
 template <typename T>
 __device__ __forceinline__ void solve(const T b[5], const CoFrame<T> &f, T a[5])
 {
-    const T R2 = fmaT(f.nU0, b[0], b[1]);
+    const T R2 = fmaT(f.nU0(), b[0], b[1]);
     const T R5 = fmaT(f.nqn, b[0], T(2.0f) * b[4]);
     a[4] = f.kal2 * fmaT(f.m2U0, R2, R5);
     a[3] = f.tl * b[3];
     a[2] = f.tl * b[2];
-    a[1] = fmaT(f.nU0, a[4], f.tl * R2);
-    a[0] = fmaT(f.nU0, a[1], fmaT(f.nqh, a[4], b[0]));
+    a[1] = fmaT(f.nU0(), a[4], f.tl * R2);
+    a[0] = fmaT(f.nU0(), a[1], fmaT(f.nqh, a[4], b[0]));
 }
 
 // M = <psi' u^k (a.psi')> over the normal table X (primed frame):

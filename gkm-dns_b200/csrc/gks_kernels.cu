@@ -565,6 +565,49 @@ struct SweepSrc {
     __device__ __forceinline__ S get_s(int i) const { return sum_s[i][threadIdx.x]; }
 };
 
+// The flux of work item `it` of field f.
+template <int DIR, typename S>
+__device__ __forceinline__ void flux_item(const FieldDev &f, long long it, S (*park_dw)[kFluxBlock],
+                                          double (*park_w)[kFluxBlock], double (*sum_d)[kFluxBlock],
+                                          S (*sum_s)[kFluxBlock])
+{
+    const Cell x = decode(unsigned(it - f.base), f);
+    unsigned cn, cs, cf, cb;
+    transverse<DIR>(x, f.flags, cn, cs, cf, cb);
+    SweepSrc<DIR, S> src;
+    src.park_dw = park_dw;
+    src.park_w = park_w;
+    src.sum_d = sum_d;
+    src.sum_s = sum_s;
+    src.load(f, x.c, along<DIR>(x, 1), cn, cs, cf, cb);
+    // collision time mu / p at the left cell (update.cpp:262-264), stored by
+    // this step's x-sweep reconstruction
+    const double tau_n = __ldg(f.tau[0] + x.c), tau_d = __ldg(f.tau[1] + x.c);
+    FluxConst fc;
+    fc.gm1 = f.gm1;
+    fc.hig = 0.5 * (f.icT * f.iR); // R / (gamma - 1) * 1 / R
+    fc.dt = f.dt;
+    fc.dx = f.dx;
+    fc.ks[0] = 2.0 * f.inv_dx;
+    fc.ks[1] = (DIR == 1 ? -0.5 : 0.5) * f.inv_dx; // y sweep: DWy = -(N - S)/(2 dx)
+    fc.ks[2] = 0.5 * f.inv_dx;
+    fc.kA = f.kA;
+    fc.K = f.K;
+    double F[5];
+    gks_flux<S>(src, tau_n, tau_d, fc, F);
+    constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
+    if (ROT) {
+        const double t = F[1];
+        F[1] = F[ROT];
+        F[ROT] = t;
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) f.F[DIR * 5 + q][x.c] = F[q];
+}
+
+// A batch of one field reads the field's descriptor from the launch
+// parameters (b.one: constant-bank operands, nothing loaded per interface);
+// an ensemble looks each interface's field up in the device array.
 template <int DIR, int PREC, int MINB>
 __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
 {
@@ -574,41 +617,16 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
     __shared__ double sum_d[10][kFluxBlock];
     __shared__ S sum_s[20][kFluxBlock];
     const long long stride = (long long)gridDim.x * blockDim.x;
+    if (b.nfields == 1) {
+        const long long end = b.hi < b.one.ncell ? b.hi : b.one.ncell; // alignment padding after the field
+        for (long long it = b.lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; it < end; it += stride)
+            flux_item<DIR, S>(b.one, it, park_dw, park_w, sum_d, sum_s);
+        return;
+    }
     for (long long it = b.lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; it < b.hi; it += stride) {
         const FieldDev &f = b.fields[field_of(b.fields, b.nfields, it)];
         if (it - f.base >= f.ncell) continue; // alignment padding after the field
-        const Cell x = decode(unsigned(it - f.base), f);
-        unsigned cn, cs, cf, cb;
-        transverse<DIR>(x, f.flags, cn, cs, cf, cb);
-        SweepSrc<DIR, S> src;
-        src.park_dw = park_dw;
-        src.park_w = park_w;
-        src.sum_d = sum_d;
-        src.sum_s = sum_s;
-        src.load(f, x.c, along<DIR>(x, 1), cn, cs, cf, cb);
-        // collision time mu / p at the left cell (update.cpp:262-264), stored by
-        // this step's x-sweep reconstruction
-        const double tau_n = __ldg(f.tau[0] + x.c), tau_d = __ldg(f.tau[1] + x.c);
-        FluxConst fc;
-        fc.gm1 = f.gm1;
-        fc.hig = 0.5 * (f.icT * f.iR); // R / (gamma - 1) * 1 / R
-        fc.dt = f.dt;
-        fc.dx = f.dx;
-        fc.ks[0] = 2.0 * f.inv_dx;
-        fc.ks[1] = (DIR == 1 ? -0.5 : 0.5) * f.inv_dx; // y sweep: DWy = -(N - S)/(2 dx)
-        fc.ks[2] = 0.5 * f.inv_dx;
-        fc.kA = f.kA;
-        fc.K = f.K;
-        double F[5];
-        gks_flux<S>(src, tau_n, tau_d, fc, F);
-        constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);
-        if (ROT) {
-            const double t = F[1];
-            F[1] = F[ROT];
-            F[ROT] = t;
-        }
-#pragma unroll
-        for (int q = 0; q < 5; ++q) f.F[DIR * 5 + q][x.c] = F[q];
+        flux_item<DIR, S>(f, it, park_dw, park_w, sum_d, sum_s);
     }
 }
 
@@ -1066,10 +1084,10 @@ cudaError_t occ(KernelT k, int block, int *n)
 // Register-cap variants (min resident blocks per SM: reconstruction blocks of
 // 128 threads at 3 / 4 / 5 -> 168 / 128 / 96 registers, each in the windowed
 // and the one-interface form, flux blocks of 64 threads at
-// 4 / 6 / 8 -> 255 / 168 / 128 registers); the tuner picks one per
+// 5 / 6 / 7 -> 204 / 168 / 146 registers); the tuner picks one per
 // kernel, precision and sweep.  Every variant gives bit-identical results.
 constexpr int kReconMinb[3] = {3, 4, 5};
-constexpr int kFluxMinb[kFluxVariants] = {4, 6, 8};
+constexpr int kFluxMinb[kFluxVariants] = {5, 6, 7};
 
 // The item range of a launch (all items of its kind when b.hi < 0) and the
 // blocks it needs: at most cfg.grid, no more than the range fills.

@@ -68,6 +68,9 @@ struct Batch {
     // work items a launch processes: [lo, hi) of the launched kernel's item
     // space; hi < 0 means all of them (the launchers fill the range in)
     long long lo = 0, hi = -1;
+    // the descriptor of a one-field batch (nfields == 1), equal to fields[0]:
+    // kernels read it from their launch parameters
+    FieldDev one;
 };
 
 // Launch configuration chosen by the tuner per kernel kind and sweep: block
