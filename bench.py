@@ -513,8 +513,15 @@ def run_ours(args):
         results[name] = {"ms": ms, "dt": dt, "clocks": clocks, "stats": s.stats(), "launch": s.launch_config()}
         solvers[name] = s
 
-    # stage timing (CUDA events around every launch) on both paths
-    stages = {name: solvers[name].time_stages(3) for name in solvers}
+    # stage timing (CUDA events around every launch) on both paths: per stage
+    # the fastest of three samples of 5 individually launched steps each
+    stages = {}
+    for name in solvers:
+        best = None
+        for _ in range(3):
+            st = solvers[name].time_stages(5)
+            best = st if best is None else {k: min(best[k], st[k]) for k in st}
+        stages[name] = best
     for name in solvers:
         solvers[name].close()
 
