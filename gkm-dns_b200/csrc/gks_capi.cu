@@ -1,8 +1,8 @@
 // C ABI of the WENO-GKS step (declarations in include/gks_b200.h).
 //
 // A context owns, per field, one device allocation of 32 * nc^3 doubles
-// (state 5, reconstruction 10, fluxes 15, mu/p 2; the statistics reuse the flux
-// arrays as scratch), the field's descriptor in a device array, and one
+// (state 5, reconstruction records 10, fluxes 15, mu/p 2; the statistics reuse
+// the flux arrays as scratch), the field's descriptor in a device array, and one
 // CUDA graph holding a whole step for all fields (seven persistent launches).
 // The reference instead allocates 50 padded arrays per rank and copies the
 // whole field host<->device every step (GPUAlloc.cu:3-17, GPUupdate.cu:74-190).
@@ -264,7 +264,7 @@ int ensure_pipe(gks_ctx *ctx, FieldHost &h)
 {
     const size_t n = (size_t)h.phys.nc * h.phys.nc * h.phys.nc;
     if (!h.pipe) {
-        if (cudaMalloc(&h.pipe, 25 * n * sizeof(double)) != cudaSuccess) {
+        if (cudaMalloc(&h.pipe, (25 * n + 2) * sizeof(double)) != cudaSuccess) {
             h.pipe = nullptr;
             return fail(ctx, GKS_ENOMEM, "pipelined-step buffers allocation failed");
         }
@@ -328,10 +328,9 @@ int evolve_pipelined(gks_ctx *ctx, double *const W[5])
     FieldDev d = h.dev;
     const size_t n = (size_t)nc * nc * nc;
     for (int q = 0; q < 5; ++q) d.Wout[q] = h.spare[q];
-    for (int q = 0; q < 10; ++q) {
-        d.rec[1][q] = h.pipe + (5 + q) * n;
-        d.rec[2][q] = h.pipe + (15 + q) * n;
-    }
+    const size_t r0 = (5 * n + 1) & ~(size_t)1; // 16-byte aligned pair arrays
+    d.rec[1] = h.pipe + r0;
+    d.rec[2] = h.pipe + r0 + 10 * n;
     CK(cudaMemcpyAsync(ctx->d_fields, &d, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream)); // the h2d stream writes the stage the last call may still read
 
@@ -490,15 +489,18 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         h.phys = phys[f];
         const gks_phys &p = phys[f];
         const long long n = (long long)p.nc * p.nc * p.nc;
-        if (cudaMalloc(&h.mem, (size_t)32 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
-        if (cudaMemset(h.mem, 0, (size_t)32 * n * sizeof(double)) != cudaSuccess) return bail(GKS_ECUDA);
+        // state 5 n, reconstruction pairs 10 n (from an even offset: 16-byte
+        // aligned), fluxes 15 n, mu/p 2 n
+        const long long r0 = (5 * n + 1) & ~1LL;
+        const size_t elems = (size_t)(r0 + 27 * n);
+        if (cudaMalloc(&h.mem, elems * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+        if (cudaMemset(h.mem, 0, elems * sizeof(double)) != cudaSuccess) return bail(GKS_ECUDA);
         FieldDev &d = h.dev;
         memset(&d, 0, sizeof(d));
         for (int q = 0; q < 5; ++q) d.W[q] = d.Wout[q] = h.mem + q * n;
-        for (int sw = 0; sw < 3; ++sw)
-            for (int q = 0; q < 10; ++q) d.rec[sw][q] = h.mem + (5 + q) * n;
-        for (int q = 0; q < 15; ++q) d.F[q] = h.mem + (15 + q) * n;
-        for (int q = 0; q < 2; ++q) d.tau[q] = h.mem + (30 + q) * n;
+        for (int sw = 0; sw < 3; ++sw) d.rec[sw] = h.mem + r0;
+        for (int q = 0; q < 15; ++q) d.F[q] = h.mem + r0 + (10 + q) * n;
+        for (int q = 0; q < 2; ++q) d.tau[q] = h.mem + r0 + (25 + q) * n;
         const int nt = p.nc + 6;
         std::vector<double> cp, inv;
         spline_coeffs(nt, cp, inv);

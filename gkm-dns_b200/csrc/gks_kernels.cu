@@ -122,6 +122,32 @@ __device__ __forceinline__ double energy(const double w[5], double T, double ri,
     return fma(w[0] * T, icT, (0.5 * ke) * ri);
 }
 
+// The reconstruction record of cell c: Wl[0..4] then Wr[0..4] as five
+// 16-byte pairs, pair k of every cell in its own array of n = nc^3 pairs
+// (rec + 2 k n doubles, 16-byte aligned): a warp's load or store of one pair
+// for 32 consecutive cells is 512 contiguous bytes, and a record takes five
+// 16-byte accesses instead of ten 8-byte ones.
+__device__ __forceinline__ void put_record(double *rec, unsigned c, const double wl[5], const double wr[5], long long n)
+{
+    double2 *p = reinterpret_cast<double2 *>(rec) + c;
+    p[0] = make_double2(wl[0], wl[1]);
+    p[n] = make_double2(wl[2], wl[3]);
+    p[2 * n] = make_double2(wl[4], wr[0]);
+    p[3 * n] = make_double2(wr[1], wr[2]);
+    p[4 * n] = make_double2(wr[3], wr[4]);
+}
+
+__device__ __forceinline__ void get_record(const double *rec, unsigned c, double v[10], long long n)
+{
+    const double2 *p = reinterpret_cast<const double2 *>(rec) + c;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const double2 t = __ldg(p + k * n);
+        v[2 * k] = t.x;
+        v[2 * k + 1] = t.y;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // WENO of one interface from its 6-cell stencil s[0..5] (LLL .. RRR) and the
 // stencil's temperatures T[0..5] (used unless GKS_DIRECT_ENERGY)
@@ -226,11 +252,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon(Batch b)
         }
         double wl[5], wr[5];
         recon_point<PREC>(s, T, direct, f.icT, wl, wr);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            f.rec[DIR][q][x.c] = wl[q];
-            f.rec[DIR][5 + q][x.c] = wr[q];
-        }
+        put_record(f.rec[DIR], x.c, wl, wr, f.ncell);
     }
 }
 
@@ -322,12 +344,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_zseg(Batch b)
             }
             double wl[5], wr[5];
             recon_point<PREC>(s, T, direct, f.icT, wl, wr);
-            const unsigned c = lbase + unsigned(k);
-#pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                f.rec[2][q][c] = wl[q];
-                f.rec[2][5 + q][c] = wr[q];
-            }
+            put_record(f.rec[2], lbase + unsigned(k), wl, wr, f.ncell);
         }
         __syncwarp();
     }
@@ -433,11 +450,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
                 for (int q = 0; q < 5; ++q) w[q] = sg(2, q);
                 store_tau(f, c, w);
             }
-#pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                f.rec[DIR][q][c] = wl[q];
-                f.rec[DIR][5 + q][c] = wr[q];
-            }
+            put_record(f.rec[DIR], c, wl, wr, f.ncell);
             // cell p + 3 + PF takes the slot of cell p + 3 + PF - NR, which no
             // stencil from here on reads (it lies below p - 2 for NR >= 5 + PF)
             fetch(p + 3 + PF);
@@ -505,19 +518,25 @@ struct SweepSrc {
     {
         // differences in double (they cancel); the flux scales them (FluxConst::ks)
         const int t = threadIdx.x;
+        const double *rec = f.rec[DIR];
+        double r0[10], rn[10], rs[10], rf[10], rb[10];
+        get_record(rec, c, r0, f.ncell);
+        get_record(rec, cn, rn, f.ncell);
+        get_record(rec, cs, rs, f.ncell);
+        get_record(rec, cf, rf, f.ncell);
+        get_record(rec, cb, rb, f.ncell);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             const int o = perm(q);
-            const double *rl = f.rec[DIR][o], *rr = f.rec[DIR][5 + o];
             const double wL = __ldg(f.W[o] + c), wR = __ldg(f.W[o] + c1);
-            const double wr = __ldg(rr + c);
-            Wl[q] = __ldg(rl + c);
+            const double wr = r0[5 + o];
+            Wl[q] = r0[o];
             DWl[0][q] = S(Wl[q] - wL);
-            DWl[1][q] = S(__ldg(rl + cn) - __ldg(rl + cs));
-            DWl[2][q] = S(__ldg(rl + cf) - __ldg(rl + cb));
+            DWl[1][q] = S(rn[o] - rs[o]);
+            DWl[2][q] = S(rf[o] - rb[o]);
             park_dw[q][t] = S(wR - wr);
-            park_dw[5 + q][t] = S(__ldg(rr + cn) - __ldg(rr + cs));
-            park_dw[10 + q][t] = S(__ldg(rr + cf) - __ldg(rr + cb));
+            park_dw[5 + q][t] = S(rn[5 + o] - rs[5 + o]);
+            park_dw[10 + q][t] = S(rf[5 + o] - rb[5 + o]);
             park_w[q][t] = wL;
             park_w[5 + q][t] = wR;
             park_w[10 + q][t] = wr;

@@ -4,10 +4,11 @@
 // Device layout of a field: five arrays of nc^3 doubles (interior cells only,
 // index (j*nc + i)*nc + k, j = y, i = x, k = z), the periodic halo being
 // applied by index wrapping inside the kernels.  Per field the context also
-// holds a reconstruction buffer (10 arrays: the left and right WENO states of
-// the interface at the high side of every cell, for the sweep in progress;
-// the slab-pipelined host step gives each sweep its own 10 arrays) and a flux
-// buffer (15 arrays: the x, y and z interface fluxes of the step).
+// holds a reconstruction buffer (the left and right WENO states of the
+// interface at the high side of every cell, for the sweep in progress: ten
+// values per cell as five arrays of 16-byte pairs; the slab-pipelined host
+// step gives each sweep its own buffer) and a flux buffer (15 arrays: the x,
+// y and z interface fluxes of the step).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -20,7 +21,8 @@ namespace gks {
 struct FieldDev {
     double *W[5];     // state, interior layout
     double *Wout[5];  // where the update writes the new state: W itself, except in the slab-pipelined host step
-    double *rec[3][10]; // per sweep x, y, z: Wl[0..4], Wr[0..4] (one shared buffer except in the pipelined step)
+    double *rec[3];   // per sweep x, y, z: five arrays of nc^3 16-byte pairs, Wl[0..4] then Wr[0..4]
+                      // (one shared buffer except in the pipelined step)
     double *F[15];    // Fx[0..4], Fy[0..4], Fz[0..4]
     double *tau[2];   // mu/p of each cell as numerator / denominator, set by the x-sweep reconstruction
     const double *spl_cp;   // natural-spline Thomas coefficients, nt entries
