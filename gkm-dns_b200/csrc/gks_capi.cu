@@ -257,7 +257,7 @@ int build_graph(gks_ctx *ctx)
 // is still read by later slabs' stencils); afterwards the two swap.  The
 // sweeps keep separate reconstruction buffers, as their slabs interleave.
 // ---------------------------------------------------------------------------
-constexpr int kPipeSlabs = 16;
+constexpr int kPipeSlabs = 24;
 constexpr int kPipeMinNc = 16;
 
 int ensure_pipe(gks_ctx *ctx, FieldHost &h)
