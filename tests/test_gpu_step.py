@@ -224,6 +224,44 @@ def test_stats_match_oracle_all_columns(gks, oracle):
     np.testing.assert_allclose(got, ref, rtol=STATS_RTOL, atol=1e-300)
 
 
+def analytic_case(nc, seed):
+    """A smooth periodic field with seeded noise, quick to build at any size:
+    density, velocity and pressure from a few integer-wavenumber modes."""
+    class C:
+        pass
+
+    c = C()
+    c.nc, c.gam, c.rho0, c.Mt, c.mu0, c.p0, c.t0, c.K = nc, 1.4, 1.0, 0.4, 2e-3, 1 / 1.4, 1.0, 2
+    c.T0 = c.p0 / (287.0 * c.rho0)
+    x = (np.arange(nc) + 0.5) * (2 * np.pi / nc)
+    Y, X, Z = x[:, None, None], x[None, :, None], x[None, None, :]  # index order (j, i, k)
+    rng = np.random.default_rng(seed)
+    noise = lambda: 1e-3 * rng.standard_normal((nc, nc, nc))  # noqa: E731
+    rho = 1.0 + 0.05 * np.sin(X + 2 * Y) * np.cos(Z) + noise()
+    # each velocity component has a skewed derivative along its own axis
+    u = 0.3 * (np.sin(X) + 0.4 * np.sin(2 * X + 0.3)) + 0.1 * np.cos(Y + 1.0) * np.sin(2 * Z) + noise()
+    v = 0.25 * (np.sin(Y) + 0.5 * np.sin(2 * Y + 1.0)) + 0.1 * np.cos(2 * X - Z) + noise()
+    w = 0.2 * (np.sin(Z) + 0.6 * np.sin(2 * Z + 0.7)) - 0.1 * np.sin(X + Y) + noise()
+    p = c.p0 * (1.0 + 0.1 * np.cos(X + Y + Z)) + noise()
+    W = np.stack([rho, rho * u, rho * v, rho * w, p / (c.gam - 1) + 0.5 * rho * (u * u + v * v + w * w)])
+    return c, gks_ic.pad_periodic(W)
+
+
+@pytest.mark.parametrize("nc", [160, 283])
+def test_stats_line_length_classes_match_oracle(gks, oracle, nc):
+    """The statistics' spline kernel picks its nodes per lane from the line
+    length nt = nc + 6 (5 up to nt = 160, 9 up to 288, 17 up to 544): 160^3
+    and 283^3 take the 9- and 17-node forms that the smaller tests do not
+    reach; every column against the oracle to 1e-10."""
+    case, W = analytic_case(nc, seed=nc)
+    prm = oracle.params(nc, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W)
+        got = s.stats_array()
+    ref = oracle.stats(W, prm)
+    np.testing.assert_allclose(got, ref, rtol=STATS_RTOL, atol=1e-300)
+
+
 @pytest.mark.parametrize("variant", ["fix_zsweep", "direct_energy", "gpu_prandtl", "power_law"])
 def test_variants_match_oracle(gks, oracle, variant):
     case = gks_ic.make_dhit(16, k0=4.0, Mt=0.5, Re_lambda=60.0, seed=9)
