@@ -547,6 +547,15 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         d.mu0 = p.mu0;
         d.visc_exp = p.visc_exp;
         d.kA = p.pr_factor * 4.0 / (p.K + 3);
+        d.hig = 0.5 * (d.icT * d.iR); // R / (gamma - 1) * 1 / R
+        d.ksn = 2.0 * d.inv_dx;
+        d.kst = 0.5 * d.inv_dx;
+        d.hK2 = (p.K + 2) * 0.5;
+        const int kint[4] = {p.K + 2, p.K + 4, (p.K + 2) * (p.K + 4), -(p.K + 3)};
+        for (int i = 0; i < 4; ++i) {
+            d.kd[i] = (double)kint[i];
+            d.kf[i] = (float)kint[i];
+        }
         // spline grid of the reference's einspline call (Interpolation.cpp:10-12)
         const double start = (0 - 3) * d.dx + 0.5 * d.dx;
         const double end = start + (nt - 1) * d.dx;

@@ -246,14 +246,24 @@ __device__ __forceinline__ Prim prim(const double W[5], double gm1, double hig)
     return p;
 }
 
-// Constants of one field that the flux needs.
+// The internal-degrees-of-freedom constants of a Maxwellian's moments in type
+// T (K = internal degrees of freedom): r2 = K + 2, q4 = K + 4,
+// r4 = (K + 2)(K + 4), nq = -(K + 3).  Precomputed per field, so that no
+// integer-to-floating conversion runs per interface.
+template <typename T> struct KConst {
+    T r2, q4, r4, nq;
+};
+
+// Constants of one field that the flux needs (all precomputed per field).
 struct FluxConst {
     double gm1;   // gamma - 1
     double hig;   // 1 / (2 (gamma - 1))
     double dt, dx;
     double ks[3]; // slope scales: 2/dx (normal), +-1/(2 dx) (transverse)
     double kA;    // pr_factor * 4 / (K + 3)
-    int K;
+    double hK2;   // (K + 2) / 2
+    KConst<double> kd; // in double and in float
+    KConst<float> kf;
 };
 
 } // namespace gks

@@ -57,8 +57,8 @@ template <typename T> struct CoFrame {
     __device__ __forceinline__ T nhu2() const { if constexpr (kDouble) return -hu2; else return nhu2_; }
 };
 
-template <typename T>
-__device__ __forceinline__ CoFrame<T> co_frame(T U0, T U1, T U2, T s, T lam, int K, T kA)
+template <typename T, typename KT>
+__device__ __forceinline__ CoFrame<T> co_frame(T U0, T U1, T U2, T s, T lam, const KConst<KT> &kc, T kA)
 {
     CoFrame<T> f;
     f.U0 = U0;
@@ -73,15 +73,15 @@ __device__ __forceinline__ CoFrame<T> co_frame(T U0, T U1, T U2, T s, T lam, int
         f.nhu2_ = m1 * f.hu2;
     }
     f.m2U0 = T(-2.0f) * U0;
-    f.nqn = fmaT(f.nU0(), U0, T(float(-(K + 3))) * s);
+    f.nqn = fmaT(f.nU0(), U0, T(kc.nq) * s);
     f.nqh = T(0.5f) * f.nqn;
     f.tl = T(2.0f) * lam;
     f.kal2 = (kA * lam) * lam;
     f.s = s;
-    f.r2 = T(float(K + 2)) * s;
+    f.r2 = T(kc.r2) * s;
     const T s2 = s * s;
-    f.q4 = T(float(K + 4)) * s2;
-    f.r4 = T(float((K + 2) * (K + 4))) * s2;
+    f.q4 = T(kc.q4) * s2;
+    f.r4 = T(kc.r4) * s2;
     return f;
 }
 
@@ -221,7 +221,7 @@ __device__ __forceinline__ Prim side_tables(const Src &src, const FluxConst &c, 
         half_table<7>(g.U0, g.s, h0, NEG ? -ex : ex, Xh);
     }
     full_table<6, double>(g.U0, g.s, Xf);
-    const double c4 = fma(0.5, fma(g.U1, g.U1, g.U2 * g.U2), double(c.K + 2) * 0.5 * g.s);
+    const double c4 = fma(0.5, fma(g.U1, g.U1, g.U2 * g.U2), c.hK2 * g.s);
     double M[5];
     mom0_lab<0>(M, Xh, g, c4);
 #pragma unroll
@@ -362,14 +362,14 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
     {
         double Xh[7], Xf[6];
         const Prim g = side_tables<0>(src, c, tw.p3, Xh, Xf);
-        const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.K, c.kA);
+        const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.kd, c.kA);
         const double sc[3] = {c.ks[0] * g.rinv, c.ks[1] * g.rinv, c.ks[2] * g.rinv};
         side_slopes<double>(SideIO64<0, Src>{src}, f, Xh, Xf, sc, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
     }
     {
         double Xh[7], Xf[6];
         const Prim g = side_tables<1>(src, c, tw.p3, Xh, Xf);
-        const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.K, c.kA);
+        const CoFrame<double> f = co_frame<double>(g.U0, g.U1, g.U2, g.s, g.lam, c.kd, c.kA);
         const double sc[3] = {c.ks[0] * g.rinv, c.ks[1] * g.rinv, c.ks[2] * g.rinv};
         side_slopes<double>(SideIO64<1, Src>{src}, f, Xh, Xf, sc, g.den, tw.w45, -tw.g5, tw.p4, -tw.p5);
     }
@@ -404,12 +404,17 @@ __device__ __forceinline__ void flux_sides(const Src &src, const FluxConst &c, c
         U0.v.y = float(g.U0); U1.v.y = float(g.U1); U2.v.y = float(g.U2);
         s.v.y = float(g.s); lam.v.y = float(g.lam); rinv.v.y = float(g.rinv); den.v.y = float(g.den);
     }
-    const CoFrame<f2> f = co_frame<f2>(U0, U1, U2, s, lam, c.K, f2(float(c.kA)));
+    const CoFrame<f2> f = co_frame<f2>(U0, U1, U2, s, lam, c.kf, f2(float(c.kA)));
     const f2 sc[3] = {f2(float(c.ks[0])) * rinv, f2(float(c.ks[1])) * rinv, f2(float(c.ks[2])) * rinv};
     side_slopes<f2>(SideIO2<Src>{src, sout}, f, Xh, Xf, sc, den, f2(float(tw.w45)), f2(float(-tw.g5)),
                     f2(float(tw.p4)), f2(float(-tw.p5)));
     asm volatile("" ::: "memory");
 }
+
+// The field's K constants in the type of the flux assembly.
+template <typename S> __device__ __forceinline__ const KConst<S> &kconst(const FluxConst &c);
+template <> __device__ __forceinline__ const KConst<double> &kconst<double>(const FluxConst &c) { return c.kd; }
+template <> __device__ __forceinline__ const KConst<float> &kconst<float>(const FluxConst &c) { return c.kf; }
 
 // Time-integrated BGK-NS flux through one interface, in the frame of the
 // interface normal.  `src` supplies the inputs when they are needed, so that
@@ -489,7 +494,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau_n, double ta
         half_table<7>(e.U0, e.s, hm, g, Xp);
         half_table<7>(e.U0, e.s, hp, -g, Xn);
     }
-    const double c4 = fma(0.5, fma(e.U1, e.U1, e.U2 * e.U2), double(c.K + 2) * 0.5 * e.s);
+    const double c4 = fma(0.5, fma(e.U1, e.U1, e.U2 * e.U2), c.hK2 * e.s);
     // B_ / rho_e in the primed frame of the equilibrium, with its nearly
     // cancelling zeroth-order part gm1 rho_e <psi>_e + gm3 W0 in double
     // (GKMflux.cpp:174-178)
@@ -502,7 +507,7 @@ __device__ __forceinline__ void gks_flux(const Src &src, double tau_n, double ta
         for (int q = 0; q < 5; ++q) Bd[q] = (fma(w, M[q], gm3 * We[q]) + double(gets(10 + q))) * e.rinv;
         to_prime<double>(Bd, -e.U1, -e.U2, -0.5 * fma(e.U1, e.U1, e.U2 * e.U2));
     }
-    const CoFrame<S> f = co_frame<S>(S(e.U0), S(e.U1), S(e.U2), S(e.s), S(e.lam), c.K, S(c.kA));
+    const CoFrame<S> f = co_frame<S>(S(e.U0), S(e.U1), S(e.U2), S(e.s), S(e.lam), kconst<S>(c), S(c.kA));
     S Xfs[6], Xps[7], Xns[7];
 #pragma unroll
     for (int n = 0; n < 6; ++n) Xfs[n] = S(Xf[n]);

@@ -604,14 +604,16 @@ __device__ __forceinline__ void flux_item(const FieldDev &f, long long it, S (*p
     const double tau_n = __ldg(f.tau[0] + x.c), tau_d = __ldg(f.tau[1] + x.c);
     FluxConst fc;
     fc.gm1 = f.gm1;
-    fc.hig = 0.5 * (f.icT * f.iR); // R / (gamma - 1) * 1 / R
+    fc.hig = f.hig;
     fc.dt = f.dt;
     fc.dx = f.dx;
-    fc.ks[0] = 2.0 * f.inv_dx;
-    fc.ks[1] = (DIR == 1 ? -0.5 : 0.5) * f.inv_dx; // y sweep: DWy = -(N - S)/(2 dx)
-    fc.ks[2] = 0.5 * f.inv_dx;
+    fc.ks[0] = f.ksn;
+    fc.ks[1] = DIR == 1 ? -f.kst : f.kst; // y sweep: DWy = -(N - S)/(2 dx)
+    fc.ks[2] = f.kst;
     fc.kA = f.kA;
-    fc.K = f.K;
+    fc.hK2 = f.hK2;
+    fc.kd = {f.kd[0], f.kd[1], f.kd[2], f.kd[3]};
+    fc.kf = {f.kf[0], f.kf[1], f.kf[2], f.kf[3]};
     double F[5];
     gks_flux<S>(src, tau_n, tau_d, fc, F);
     constexpr int ROT = DIR == 0 ? 0 : (DIR == 1 ? 2 : 3);

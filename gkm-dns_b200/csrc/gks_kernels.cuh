@@ -46,6 +46,12 @@ struct FieldDev {
     double T0, iT0, mu0, visc_exp;
     double kA;        // pr_factor * 4/(K+3)
     double spl_s;     // 3/h of the spline grid
+    // flux constants computed once on the host (no per-interface conversions
+    // or products): 1/(2 (gam-1)), slope scales 2/dx and 1/(2 dx), (K+2)/2,
+    // and K + 2, K + 4, (K+2)(K+4), -(K+3) in double and in float
+    double hig, ksn, kst, hK2;
+    double kd[4];
+    float kf[4];
 };
 
 // Field item ranges start at multiples of this, so that a block of up to
