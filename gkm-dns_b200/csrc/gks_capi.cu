@@ -334,6 +334,13 @@ int evolve_pipelined(gks_ctx *ctx, double *const W[5])
     CK(cudaMemcpyAsync(ctx->d_fields, &d, sizeof(FieldDev), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream)); // the h2d stream writes the stage the last call may still read
 
+    // the caller's five arrays one after another (a (5, nt, nt, nt) block) and a
+    // pitch the copy engine accepts: one pitched copy per slab and direction
+    int max_pitch = 0;
+    CK(cudaDeviceGetAttribute(&max_pitch, cudaDevAttrMaxPitch, ctx->device));
+    const size_t pitch = (size_t)Nt * sizeof(double);
+    bool contiguous = pitch <= (size_t)max_pitch;
+    for (int q = 1; q < 5 && contiguous; ++q) contiguous = W[q] == W[0] + q * Nt;
     // slabs in unwrapped planes: [-3, 0), then [(k-1) S, min(k S, nc-3))
     const long long S = (nc - 3 + kPipeSlabs - 1) / kPipeSlabs;
     std::vector<std::pair<long long, long long>> slabs{{-3, 0}};
@@ -360,11 +367,22 @@ int evolve_pipelined(gks_ctx *ctx, double *const W[5])
     for (size_t k = 0; k < slabs.size(); ++k) {
         const long long a = slabs[k].first, b = slabs[k].second;
         const bool all = k + 1 == slabs.size();
-        // upload: padded planes of unwrapped [a, b) (physical planes + 3), one copy per component
+        // upload: padded planes of unwrapped [a, b) (physical planes + 3): one
+        // pitched copy of five rows when the caller's components lie one after
+        // another in one block, else one copy per component
         int r = phys(a, b, [&](long long p0, long long p1) -> int {
+            const size_t off = (size_t)(p0 + 3) * P, bytes = (size_t)(p1 - p0) * P * sizeof(double);
+            if (contiguous) {
+                // refused when the block is page-locked in several pieces (one
+                // registration per component): copy per component from here on
+                if (cudaMemcpy2DAsync(ctx->d_stage + off, pitch, W[0] + off, pitch, bytes, 5, cudaMemcpyHostToDevice,
+                                      ctx->h2d) == cudaSuccess)
+                    return GKS_OK;
+                cudaGetLastError();
+                contiguous = false;
+            }
             for (int q = 0; q < 5; ++q)
-                CK(cudaMemcpyAsync(ctx->d_stage + q * Nt + (p0 + 3) * P, W[q] + (p0 + 3) * P,
-                                   (size_t)(p1 - p0) * P * sizeof(double), cudaMemcpyHostToDevice, ctx->h2d));
+                CK(cudaMemcpyAsync(ctx->d_stage + q * Nt + off, W[q] + off, bytes, cudaMemcpyHostToDevice, ctx->h2d));
             return GKS_OK;
         });
         if (r) return r;
@@ -417,9 +435,16 @@ int evolve_pipelined(gks_ctx *ctx, double *const W[5])
         }
         for (auto pr : rng) {
             if (pr.second <= pr.first) continue;
+            const size_t off = (size_t)pr.first * P, bytes = (size_t)(pr.second - pr.first) * P * sizeof(double);
+            if (contiguous) {
+                if (cudaMemcpy2DAsync(W[0] + off, pitch, ctx->d_stage_out + off, pitch, bytes, 5,
+                                      cudaMemcpyDeviceToHost, ctx->d2h) == cudaSuccess)
+                    continue;
+                cudaGetLastError();
+                contiguous = false;
+            }
             for (int q = 0; q < 5; ++q)
-                CK(cudaMemcpyAsync(W[q] + pr.first * P, ctx->d_stage_out + q * Nt + pr.first * P,
-                                   (size_t)(pr.second - pr.first) * P * sizeof(double), cudaMemcpyDeviceToHost,
+                CK(cudaMemcpyAsync(W[q] + off, ctx->d_stage_out + q * Nt + off, bytes, cudaMemcpyDeviceToHost,
                                    ctx->d2h));
         }
     }

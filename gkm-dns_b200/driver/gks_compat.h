@@ -60,10 +60,17 @@ public:
         for (int q = 0; q < 5 && same; ++q) same = pinned[q] == (void *)W[q];
         if (same) return;
         unpin();
-        for (int q = 0; q < 5; ++q) {
-            int made = 0;
-            // a failure leaves W pageable: the copies still work, overlapping less
-            if (gks_host_register(W[q], bytes, &made) == GKS_OK && made) pinned[q] = W[q];
+        // one range when the five arrays lie one after another (then each slab
+        // moves in one pitched copy per direction), else one per array; a
+        // failure leaves W pageable: the copies still work, overlapping less
+        bool block = true;
+        for (int q = 1; q < 5 && block; ++q) block = W[q] == W[0] + (size_t)q * Nt_seg;
+        int made = 0;
+        if (block) {
+            if (gks_host_register(W[0], 5 * bytes, &made) == GKS_OK && made) pinned[0] = W[0];
+        } else {
+            for (int q = 0; q < 5; ++q)
+                if (gks_host_register(W[q], bytes, &made) == GKS_OK && made) pinned[q] = W[q];
         }
         pinned_bytes = bytes;
 #else

@@ -115,7 +115,10 @@ int gks_download(gks_ctx *ctx, int f, double *const W[5]);
  * one copy stream, each slab's stages run as soon as the planes they read
  * have arrived, and updated planes come back on another copy stream -- with W
  * in pinned (page-locked) host memory both PCIe directions and the kernels
- * run concurrently; pageable W works but overlaps less.  The first such call
+ * run concurrently; pageable W works but overlaps less.  When the five arrays
+ * lie one after another in one block (W[q] = W[0] + q (nc+6)^3), each slab
+ * moves in one pitched copy per direction instead of five; page-lock such a
+ * block as one range (gks_host_register) to keep that.  The first such call
  * allocates 25 nc^3 + 5 (nc+6)^3 doubles of pipeline buffers for the context
  * (4.1 GB at 256^3).  Otherwise (an ensemble, nsteps > 1, nc < 16) it is
  * gks_upload + gks_step + gks_download.  Results are bit-identical either way. */

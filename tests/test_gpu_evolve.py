@@ -125,3 +125,22 @@ def test_host_register_pins_a_pageable_field(gks):
         for p in ptrs:
             assert lib.gks_host_unregister(ctypes.c_void_p(p)) == 0
     assert lib.gks_host_register(None, 8, None) == -1
+
+
+def test_evolve_with_separate_component_arrays(gks):
+    """The five host arrays need not be one block: separately allocated
+    components take one copy per component and slab instead of one pitched
+    copy, with the same result."""
+    import ctypes
+
+    nc = 40
+    case = gks_ic.make_dhit(nc, k0=4.0, Mt=0.4, seed=11)
+    W0 = gks_ic.to_conservative_padded(case)
+    comps = [np.ascontiguousarray(W0[q]).copy() for q in range(5)]  # five separate allocations
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W0)
+        dt = s.timestep(0.5)
+        ptrs = gks.DP5(*[c.ctypes.data_as(gks.DP) for c in comps])
+        rc = gks.load_library().gks_evolve(s._h, 0, ptrs, 1)
+        assert rc == 0
+    assert np.array_equal(np.stack(comps), plain(gks, case, W0, gks.FP64, dt))
