@@ -316,12 +316,36 @@ int pipe_stage(gks_ctx *ctx, const FieldDev &d, int kind, int dir, long long p0,
     return GKS_OK;
 }
 
+int evolve_slabs(gks_ctx *ctx, double *const W[5]);
+
 int evolve_pipelined(gks_ctx *ctx, double *const W[5])
 {
     FieldHost &h = ctx->fh[0];
     int rc = ensure_stage(ctx, 0);
     if (!rc) rc = ensure_pipe(ctx, h);
     if (rc) return rc;
+    rc = evolve_slabs(ctx, W);
+    if (rc != GKS_OK) {
+        // drain what was enqueued and put the field's own descriptor back, so
+        // that later work reads and writes the field's state buffers; their
+        // contents are undefined until the next upload
+        cudaStreamSynchronize(ctx->h2d);
+        cudaStreamSynchronize(ctx->d2h);
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        cudaMemcpy(ctx->d_fields, &h.dev, sizeof(FieldDev), cudaMemcpyHostToDevice);
+        ctx->batch.one = h.dev;
+        drop_graph(ctx);
+        h.uploaded = false;
+    }
+    return rc;
+}
+
+// The pipelined step proper (see above); the caller restores the field's
+// descriptor if it fails.
+int evolve_slabs(gks_ctx *ctx, double *const W[5])
+{
+    FieldHost &h = ctx->fh[0];
     const long long nc = h.phys.nc, nt = nc + 6, P = nt * nt, Nt = P * nt, plane = nc * nc;
     // descriptor of this step: reads the uploaded state, writes the spare,
     // the y and z sweeps into their own reconstruction buffers

@@ -121,7 +121,8 @@ int gks_download(gks_ctx *ctx, int f, double *const W[5]);
  * block as one range (gks_host_register) to keep that.  The first such call
  * allocates 25 nc^3 + 5 (nc+6)^3 doubles of pipeline buffers for the context
  * (4.1 GB at 256^3).  Otherwise (an ensemble, nsteps > 1, nc < 16) it is
- * gks_upload + gks_step + gks_download.  Results are bit-identical either way. */
+ * gks_upload + gks_step + gks_download.  Results are bit-identical either way.
+ * After a failure the field's device state is undefined: upload it again. */
 int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps);
 
 /* Page-lock `bytes` of caller memory at p (cudaHostRegister) so that copies
