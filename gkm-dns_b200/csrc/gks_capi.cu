@@ -30,6 +30,11 @@ struct FieldHost {
     FieldDev dev;
     double *mem = nullptr;
     double *spl = nullptr;
+    // one y-slab of a field split over ranks (gks_create_slab): its interior
+    // planes, and the four halo buffers of 15 nc^2 doubles each (send south,
+    // send north, receive south, receive north)
+    int slab = 0;
+    double *halo = nullptr;
     // slab-pipelined host step (gks_evolve): one allocation of 25 nc^3 doubles
     // -- the spare state the step writes (5) and the y and z sweeps' own
     // reconstruction buffers (10 + 10) -- made on first use
@@ -120,10 +125,18 @@ void spline_coeffs(int nt, std::vector<double> &cp, std::vector<double> &inv)
     }
 }
 
+// Doubles of the padded host layout of field f: 5 x nty x nt^2 (nty = nt, or
+// the slab's planes with their ghosts).
+size_t host_elems(const gks_ctx *ctx, int f)
+{
+    const FieldDev &d = ctx->fh[f].dev;
+    const size_t nt = (size_t)d.nc + 6;
+    return 5 * (size_t)(d.ny + 2 * d.yhost) * nt * nt;
+}
+
 int ensure_stage(gks_ctx *ctx, int f)
 {
-    const size_t nt = (size_t)ctx->fh[f].phys.nc + 6;
-    const size_t need = 5 * nt * nt * nt;
+    const size_t need = host_elems(ctx, f);
     if (ctx->stage_elems >= need) return GKS_OK;
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     ctx->d_stage = nullptr;
@@ -206,8 +219,11 @@ std::string tune_key(const gks_ctx *ctx)
     return k;
 }
 
+int record_slab_step(gks_ctx *ctx);
+
 int record_step(gks_ctx *ctx)
 {
+    if (ctx->fh[0].slab) return record_slab_step(ctx);
     for (int dir = 0; dir < 3; ++dir) {
         CK(gks::launch_recon(ctx->batch, dir, ctx->precision, ctx->cfg[gks::K_RECON][dir], ctx->stream));
         CK(gks::launch_flux(ctx->batch, dir, ctx->precision, ctx->cfg[gks::K_FLUX][dir], ctx->stream));
@@ -314,6 +330,30 @@ int pipe_stage(gks_ctx *ctx, const FieldDev &d, int kind, int dir, long long p0,
     else if (kind == gks::K_FLUX) CK(gks::launch_flux(b, dir, ctx->precision, c, ctx->stream));
     else CK(gks::launch_update(b, c, ctx->stream));
     return GKS_OK;
+}
+
+// One step of a y-slab (gks_create_slab): ranged launches over its stored
+// planes j = 0 .. ny+5 (the ny interior planes 3 .. ny+2 and three ghost
+// planes either side, which the halo exchange filled):
+//   x, z reconstruction  planes [2, ny+4)  (the x / z fluxes' transverse
+//                                           neighbours; mu/p of plane 2)
+//   x, z flux            planes [3, ny+3)
+//   y reconstruction     planes [2, ny+3)  (interface j + 1/2: cells j-2 .. j+3)
+//   y flux               planes [2, ny+3)
+//   update               planes [3, ny+3)  (Fy of planes j-1 and j)
+// Every stage reads planes inside [0, ny+6) only: the y index never wraps.
+int record_slab_step(gks_ctx *ctx)
+{
+    const FieldDev &d = ctx->fh[0].dev;
+    const long long S = ctx->fh[0].slab;
+    int rc;
+    if ((rc = pipe_stage(ctx, d, gks::K_RECON, 0, 2, S + 4))) return rc;
+    if ((rc = pipe_stage(ctx, d, gks::K_FLUX, 0, 3, S + 3))) return rc;
+    if ((rc = pipe_stage(ctx, d, gks::K_RECON, 1, 2, S + 3))) return rc;
+    if ((rc = pipe_stage(ctx, d, gks::K_FLUX, 1, 2, S + 3))) return rc;
+    if ((rc = pipe_stage(ctx, d, gks::K_RECON, 2, 2, S + 4))) return rc;
+    if ((rc = pipe_stage(ctx, d, gks::K_FLUX, 2, 3, S + 3))) return rc;
+    return pipe_stage(ctx, d, gks::K_UPDATE, 0, 3, S + 3);
 }
 
 int evolve_slabs(gks_ctx *ctx, double *const W[5]);
@@ -494,7 +534,13 @@ extern "C" {
 
 const char *gks_last_error(const gks_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
-int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, int flags)
+} // extern "C"
+
+namespace {
+
+// A context of `nfields` periodic fields, or (slab > 0, one field) of the
+// y-slab of `slab` interior planes starting at global plane y0.
+int create_ctx(gks_ctx **out, int nfields, const gks_phys *phys, int precision, int flags, int slab, int y0)
 {
     if (!out || nfields < 1 || !phys) return GKS_EINVAL;
     *out = nullptr;
@@ -528,7 +574,7 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     for (; run > gks::kWinRunMin; run /= 2) {
         long long items = 0;
         for (int f = 0; f < nfields; ++f)
-            items += (long long)phys[f].nc * phys[f].nc * ((phys[f].nc + run - 1) / run);
+            items += (long long)(slab ? slab + 6 : phys[f].nc) * phys[f].nc * ((phys[f].nc + run - 1) / run);
         if (items >= (long long)gks::kWinItemsPerSm * ctx->nsm) break;
     }
     long long base = 0, wbase = 0, zbase = 0;
@@ -536,8 +582,10 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     for (int f = 0; f < nfields; ++f) {
         FieldHost &h = ctx->fh[f];
         h.phys = phys[f];
+        h.slab = slab;
         const gks_phys &p = phys[f];
-        const long long n = (long long)p.nc * p.nc * p.nc;
+        const int ny = slab ? slab + 6 : p.nc; // stored planes
+        const long long n = (long long)ny * p.nc * p.nc;
         // state 5 n, reconstruction pairs 10 n (from an even offset: 16-byte
         // aligned), fluxes 15 n, mu/p 2 n
         const long long r0 = (5 * n + 1) & ~1LL;
@@ -550,24 +598,40 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
         for (int sw = 0; sw < 3; ++sw) d.rec[sw] = h.mem + r0;
         for (int q = 0; q < 15; ++q) d.F[q] = h.mem + r0 + (10 + q) * n;
         for (int q = 0; q < 2; ++q) d.tau[q] = h.mem + r0 + (25 + q) * n;
-        const int nt = p.nc + 6;
-        std::vector<double> cp, inv;
-        spline_coeffs(nt, cp, inv);
-        if (cudaMalloc(&h.spl, 2 * (size_t)nt * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
-        if (cudaMemcpy(h.spl, cp.data(), nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h.spl + nt, inv.data(), nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-            return bail(GKS_ECUDA);
+        // spline coefficients: x / z lines of nt nodes, y lines of nty (a
+        // slab's own when it is a slab)
+        const int nt = p.nc + 6, nty = slab ? ny : nt;
+        const size_t nspl = 2 * (size_t)nt + (slab ? 2 * (size_t)nty : 0);
+        if (cudaMalloc(&h.spl, nspl * sizeof(double)) != cudaSuccess) return bail(GKS_ENOMEM);
+        for (int a = 0; a < (slab ? 2 : 1); ++a) {
+            const int m = a ? nty : nt;
+            double *dst = h.spl + (a ? 2 * (size_t)nt : 0);
+            std::vector<double> cp, inv;
+            spline_coeffs(m, cp, inv);
+            if (cudaMemcpy(dst, cp.data(), m * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(dst + m, inv.data(), m * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+                return bail(GKS_ECUDA);
+        }
         d.spl_cp = h.spl;
         d.spl_inv = h.spl + nt;
+        d.spl_cpy = slab ? h.spl + 2 * nt : d.spl_cp;
+        d.spl_invy = slab ? h.spl + 2 * nt + nty : d.spl_inv;
+        d.ny = ny;
+        d.nyw = slab ? gks::kNoWrap : p.nc;
+        d.yhost = slab ? 0 : 3;
+        d.ylo = slab ? 3 : 0;
+        d.yhi = slab ? slab + 3 : p.nc;
+        if (slab && cudaMalloc(&h.halo, 4 * 15 * (size_t)p.nc * p.nc * sizeof(double)) != cudaSuccess)
+            return bail(GKS_ENOMEM);
         d.base = base;
         d.ncell = n;
         base += (n + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
         d.run = run;
         d.nrun = (p.nc + run - 1) / run;
-        d.nwin = (long long)p.nc * p.nc * d.nrun;
+        d.nwin = (long long)ny * p.nc * d.nrun;
         d.wbase = wbase;
         wbase += (d.nwin + gks::kItemAlign - 1) / gks::kItemAlign * gks::kItemAlign;
-        d.nzseg = (long long)p.nc * p.nc * ((p.nc + 31) / 32);
+        d.nzseg = (long long)ny * p.nc * ((p.nc + 31) / 32);
         d.zbase = zbase;
         zbase += d.nzseg;
         d.nc = p.nc;
@@ -605,10 +669,16 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
             d.kd[i] = (double)kint[i];
             d.kf[i] = (float)kint[i];
         }
-        // spline grid of the reference's einspline call (Interpolation.cpp:10-12)
-        const double start = (0 - 3) * d.dx + 0.5 * d.dx;
-        const double end = start + (nt - 1) * d.dx;
-        d.spl_s = 3.0 / ((end - start) / (double)(nt - 1));
+        // spline grids of the reference's einspline call (Interpolation.cpp:10-27):
+        // a segment's grid starts at its first plane sta, here 0 along x and z
+        // and y0 along y
+        auto scale = [&](int sta, int num) {
+            const double start = (sta - 3) * d.dx + 0.5 * d.dx;
+            const double end = start + (num - 1) * d.dx;
+            return 3.0 / ((end - start) / (double)(num - 1));
+        };
+        d.spl_s = scale(0, nt);
+        d.spl_sy = scale(slab ? y0 : 0, nty);
     }
     if (cudaMalloc(&ctx->d_fields, nfields * sizeof(FieldDev)) != cudaSuccess) return bail(GKS_ENOMEM);
     for (int f = 0; f < nfields; ++f)
@@ -633,6 +703,23 @@ int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, 
     return GKS_OK;
 }
 
+} // namespace
+
+extern "C" {
+
+int gks_create(gks_ctx **out, int nfields, const gks_phys *phys, int precision, int flags)
+{
+    return create_ctx(out, nfields, phys, precision, flags, 0, 0);
+}
+
+int gks_create_slab(gks_ctx **out, const gks_phys *phys, int ny, int y0, int precision, int flags)
+{
+    if (!out || !phys) return GKS_EINVAL;
+    *out = nullptr;
+    if (ny < 3 || ny > phys->nc || y0 < 0 || y0 + ny > phys->nc) return GKS_EINVAL;
+    return create_ctx(out, 1, phys, precision, flags, ny, y0);
+}
+
 void gks_destroy(gks_ctx *ctx)
 {
     if (!ctx) return;
@@ -643,6 +730,7 @@ void gks_destroy(gks_ctx *ctx)
         if (h.mem) cudaFree(h.mem);
         if (h.spl) cudaFree(h.spl);
         if (h.pipe) cudaFree(h.pipe);
+        if (h.halo) cudaFree(h.halo);
     }
     if (ctx->d_fields) cudaFree(ctx->d_fields);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
@@ -668,7 +756,7 @@ int gks_upload(gks_ctx *ctx, int f, double *const W[5])
         if (!W[q]) return fail(ctx, GKS_EINVAL, "null component pointer");
     CK(cudaSetDevice(ctx->device));
     if ((rc = ensure_stage(ctx, f))) return rc;
-    const size_t nt = (size_t)ctx->fh[f].phys.nc + 6, Nt = nt * nt * nt;
+    const size_t Nt = host_elems(ctx, f) / 5;
     for (int q = 0; q < 5; ++q)
         CK(cudaMemcpyAsync(ctx->d_stage + q * Nt, W[q], Nt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(gks::launch_gather(ctx->fh[f].dev, ctx->d_stage, ctx->nsm, ctx->stream));
@@ -686,7 +774,7 @@ int gks_download(gks_ctx *ctx, int f, double *const W[5])
         if (!W[q]) return fail(ctx, GKS_EINVAL, "null component pointer");
     CK(cudaSetDevice(ctx->device));
     if ((rc = ensure_stage(ctx, f))) return rc;
-    const size_t nt = (size_t)ctx->fh[f].phys.nc + 6, Nt = nt * nt * nt;
+    const size_t Nt = host_elems(ctx, f) / 5;
     CK(gks::launch_scatter(ctx->fh[f].dev, ctx->d_stage, ctx->nsm, ctx->stream));
     for (int q = 0; q < 5; ++q)
         CK(cudaMemcpyAsync(W[q], ctx->d_stage + q * Nt, Nt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -704,7 +792,8 @@ int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps)
     if (nsteps < 1) return fail(ctx, GKS_EINVAL, "nsteps must be at least 1");
     if (!ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "evolve before dt of field " + std::to_string(f));
     CK(cudaSetDevice(ctx->device));
-    if (ctx->nfields == 1 && nsteps == 1 && ctx->fh[f].phys.nc >= kPipeMinNc) return evolve_pipelined(ctx, W);
+    if (ctx->nfields == 1 && nsteps == 1 && ctx->fh[f].phys.nc >= kPipeMinNc && !ctx->fh[f].slab)
+        return evolve_pipelined(ctx, W);
     // several fields or steps: upload, the captured steps, download
     if ((rc = gks_upload(ctx, f, W))) return rc;
     for (int g = 0; g < ctx->nfields; ++g)
@@ -813,20 +902,45 @@ int gks_check(gks_ctx *ctx)
     return GKS_OK;
 }
 
-int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
+int gks_stats_part(gks_ctx *ctx, int f, double *part)
 {
     int rc = check_field(ctx, f);
     if (rc) return rc;
-    if (!out) return fail(ctx, GKS_EINVAL, "null output");
+    if (!part) return fail(ctx, GKS_EINVAL, "null output");
     if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "stats before upload");
     CK(cudaSetDevice(ctx->device));
     const FieldDev &d = ctx->fh[f].dev;
     CK(gks::launch_stats(d, d.F[0], ctx->d_partial, ctx->d_sums, ctx->nsm, ctx->stream));
-    double s[24];
-    CK(cudaMemcpyAsync(s, ctx->d_sums, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(part, ctx->d_sums, 27 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const gks_phys &p = ctx->fh[f].phys;
-    // PrintStats normalisation (update.cpp:727-776); s[0..23] are means already
+    part[27] = double(d.yhi - d.ylo) * d.nc * d.nc;
+    return GKS_OK;
+}
+
+int gks_stats_reduce(const double *parts, int nparts, const gks_phys *phys, gks_stats_out *out)
+{
+    if (!parts || nparts < 1 || !phys || !out) return GKS_EINVAL;
+    // cell-weighted means of the parts (MPI_Reduce / MPI_Allreduce of the
+    // sums, update.cpp:714-741); the shifted moments of p, T and 1/rho move
+    // to the first part's shift K: with e = K_r - K,
+    //   E[x - K] = E[x - K_r] + e,  E[(x - K)^2] = E[(x - K_r)^2] + 2 e E[x - K_r] + e^2
+    double N = 0.0;
+    for (int r = 0; r < nparts; ++r) {
+        if (!(parts[28 * r + 27] > 0.0)) return GKS_EINVAL;
+        N += parts[28 * r + 27];
+    }
+    double s[24] = {};
+    for (int r = 0; r < nparts; ++r) {
+        const double *m = parts + 28 * r, w = m[27] / N;
+        for (int i = 0; i < 18; ++i) s[i] += w * m[i];
+        for (int x = 0; x < 3; ++x) {
+            const double e = m[24 + x] - parts[24 + x], m1 = m[18 + 2 * x], m2 = m[19 + 2 * x];
+            s[18 + 2 * x] += w * (m1 + e);
+            s[19 + 2 * x] += w * (m2 + (2.0 * e * m1 + e * e));
+        }
+    }
+    const gks_phys &p = *phys;
+    // PrintStats normalisation (update.cpp:727-776)
     out->tke = s[0];
     out->diss = s[1];
     out->sijsij = s[2];
@@ -844,6 +958,92 @@ int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
     out->mach_t = std::sqrt(s[15]) / s[16];
     out->rho_mean = s[17];
     return GKS_OK;
+}
+
+int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
+{
+    double part[28];
+    int rc = gks_stats_part(ctx, f, part);
+    if (rc) return rc;
+    if (!out) return fail(ctx, GKS_EINVAL, "null output");
+    return gks_stats_reduce(part, 1, &ctx->fh[f].phys, out);
+}
+
+int gks_halo_buffers(gks_ctx *ctx, double **bufs, size_t *elems)
+{
+    if (!ctx || !bufs) return GKS_EINVAL;
+    const FieldHost &h = ctx->fh[0];
+    if (!h.slab) return fail(ctx, GKS_EINVAL, "halo buffers belong to a slab context");
+    const size_t m = 15 * (size_t)h.phys.nc * h.phys.nc;
+    for (int i = 0; i < 4; ++i) bufs[i] = h.halo + i * m;
+    if (elems) *elems = m;
+    return GKS_OK;
+}
+
+} // extern "C"
+
+namespace {
+
+// Three planes [j0, j0 + 3) of the five components <-> a halo buffer laid out
+// [component][plane][nc^2]: one pitched copy when the components lie evenly
+// spaced in one allocation (as gks_create_slab lays them out), else one copy
+// per component.
+int halo_copy(gks_ctx *ctx, long long j0, double *buf, bool to_buf)
+{
+    const FieldHost &h = ctx->fh[0];
+    const size_t P = (size_t)h.phys.nc * h.phys.nc, n = (size_t)h.dev.ncell, width = 3 * P * sizeof(double);
+    bool even = true;
+    for (int q = 1; q < 5; ++q) even = even && h.dev.W[q] == h.dev.W[0] + q * n;
+    int max_pitch = 0;
+    CK(cudaDeviceGetAttribute(&max_pitch, cudaDevAttrMaxPitch, ctx->device));
+    if (even && n * sizeof(double) <= (size_t)max_pitch) {
+        double *st = h.dev.W[0] + j0 * P;
+        if (to_buf)
+            CK(cudaMemcpy2DAsync(buf, width, st, n * sizeof(double), width, 5, cudaMemcpyDeviceToDevice, ctx->stream));
+        else
+            CK(cudaMemcpy2DAsync(st, n * sizeof(double), buf, width, width, 5, cudaMemcpyDeviceToDevice, ctx->stream));
+        return GKS_OK;
+    }
+    for (int q = 0; q < 5; ++q) {
+        double *st = h.dev.W[q] + j0 * P, *b = buf + q * 3 * P;
+        CK(cudaMemcpyAsync(to_buf ? b : st, to_buf ? st : b, width, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return GKS_OK;
+}
+
+int halo_ready(gks_ctx *ctx)
+{
+    if (!ctx) return GKS_EINVAL;
+    if (!ctx->fh[0].slab) return fail(ctx, GKS_EINVAL, "halo exchange belongs to a slab context");
+    if (!ctx->fh[0].uploaded) return fail(ctx, GKS_ESTATE, "halo exchange before upload");
+    CK(cudaSetDevice(ctx->device));
+    return GKS_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int gks_halo_pack(gks_ctx *ctx)
+{
+    int rc = halo_ready(ctx);
+    if (rc) return rc;
+    double *b[4];
+    gks_halo_buffers(ctx, b, nullptr);
+    const long long S = ctx->fh[0].slab;
+    if ((rc = halo_copy(ctx, 3, b[0], true))) return rc; // south: the first three interior planes
+    return halo_copy(ctx, S, b[1], true);                // north: the last three
+}
+
+int gks_halo_unpack(gks_ctx *ctx)
+{
+    int rc = halo_ready(ctx);
+    if (rc) return rc;
+    double *b[4];
+    gks_halo_buffers(ctx, b, nullptr);
+    const long long S = ctx->fh[0].slab;
+    if ((rc = halo_copy(ctx, 0, b[2], false))) return rc; // from the south neighbour's north planes
+    return halo_copy(ctx, S + 3, b[3], false);             // from the north neighbour's south planes
 }
 
 int gks_device_fields(gks_ctx *ctx, int f, double *dW[5])
@@ -881,6 +1081,7 @@ int gks_select_device(int device)
 int gks_time_stages(gks_ctx *ctx, int reps, double *ms)
 {
     if (!ctx || !ms || reps < 1) return GKS_EINVAL;
+    if (ctx->fh[0].slab) return fail(ctx, GKS_EINVAL, "stage timing runs whole-field launches: not for a slab");
     for (int f = 0; f < ctx->nfields; ++f)
         if (!ctx->fh[f].uploaded || !ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "time_stages before upload/dt");
     CK(cudaSetDevice(ctx->device));
@@ -916,6 +1117,9 @@ int gks_time_stages(gks_ctx *ctx, int reps, double *ms)
 int gks_autotune(gks_ctx *ctx, int reps)
 {
     if (!ctx || reps < 1) return GKS_EINVAL;
+    if (ctx->fh[0].slab)
+        return fail(ctx, GKS_EINVAL, "the tuner times whole-field launches: tune a periodic field of the same edge "
+                                     "and pin its choice on the slab (gks_set_launch)");
     for (int f = 0; f < ctx->nfields; ++f)
         if (!ctx->fh[f].uploaded || !ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "autotune before upload/dt");
     CK(cudaSetDevice(ctx->device));

@@ -34,6 +34,7 @@ __device__ __forceinline__ int field_of(const FieldDev *f, int n, long long it)
 
 struct Cell {
     int j, i, k, nc;
+    int nyw;    // y-wrap modulus (FieldDev::nyw)
     unsigned c; // (j*nc + i)*nc + k
 };
 
@@ -47,6 +48,7 @@ __device__ __forceinline__ Cell decode(unsigned c, const FieldDev &f)
 {
     Cell x;
     x.nc = f.nc;
+    x.nyw = f.nyw;
     x.c = c;
     const unsigned r = div_nc(c, f);
     x.k = int(c - r * f.nc);
@@ -59,13 +61,14 @@ __device__ __forceinline__ Cell decode(unsigned c, const FieldDev &f)
 __device__ __forceinline__ int wrap(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 
 // Displacement along the sweep axis: DIR 0 = x (i), 1 = y (j), 2 = z (k);
-// only the swept coordinate wraps.
+// only the swept coordinate wraps (y not at all in a slab, whose ghost planes
+// are stored).
 template <int DIR>
 __device__ __forceinline__ unsigned along(const Cell &x, int d)
 {
     const int n = x.nc;
     if (DIR == 0) return x.c + (unsigned)((wrap(x.i + d, n) - x.i) * n);
-    if (DIR == 1) return x.c + (unsigned)((wrap(x.j + d, n) - x.j) * n * n);
+    if (DIR == 1) return x.c + (unsigned)((wrap(x.j + d, x.nyw) - x.j) * n * n);
     return x.c + (unsigned)(wrap(x.k + d, n) - x.k);
 }
 
@@ -406,7 +409,7 @@ __global__ void __launch_bounds__(kReconBlock, MINB) k_recon_win(Batch b)
         const unsigned step = DIR == 0 ? unsigned(nc) : unsigned(nc) * unsigned(nc);
         const unsigned lbase = DIR == 0 ? unsigned(line) * unsigned(nc) * unsigned(nc) + unsigned(k)
                                         : unsigned(line) * unsigned(nc) + unsigned(k);
-        auto cell = [&](int p) -> unsigned { return lbase + unsigned(wrap(p, nc)) * step; };
+        auto cell = [&](int p) -> unsigned { return lbase + unsigned(wrap(p, DIR == 0 ? nc : f.nyw)) * step; };
         const bool direct = (f.flags & GKS_DIRECT_ENERGY) != 0;
         // cells of the run's stencils: s0 - 2 .. last (unwrapped, at most nc + 2),
         // cell pc in ring slot pc mod NR, one copy group per cell (empty past the run)
@@ -689,11 +692,11 @@ __global__ void __launch_bounds__(kUpdateBlock) k_update(Batch b)
 __global__ void k_gather(FieldDev f, const double *__restrict__ stage, long long lo, long long hi)
 {
     const int nc = f.nc, nt = nc + 6;
-    const long long Nt = (long long)nt * nt * nt;
+    const long long Nt = (long long)(f.ny + 2 * f.yhost) * nt * nt;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; c < hi; c += stride) {
         const Cell x = decode(unsigned(c), f);
-        const long long p = ((long long)(x.j + 3) * nt + (x.i + 3)) * nt + (x.k + 3);
+        const long long p = ((long long)(x.j + f.yhost) * nt + (x.i + 3)) * nt + (x.k + 3);
 #pragma unroll
         for (int q = 0; q < 5; ++q) f.W[q][c] = stage[q * Nt + p];
     }
@@ -702,13 +705,13 @@ __global__ void k_gather(FieldDev f, const double *__restrict__ stage, long long
 __global__ void k_scatter(FieldDev f, double *__restrict__ stage, long long lo, long long hi)
 {
     const int nc = f.nc, nt = nc + 6;
-    const long long Nt = (long long)nt * nt * nt;
+    const long long Nt = (long long)(f.ny + 2 * f.yhost) * nt * nt;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long p = lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += stride) {
         const int kk = int(p % nt);
         const int ii = int((p / nt) % nt);
         const int jj = int(p / ((long long)nt * nt));
-        const long long c = ((long long)wrap(jj - 3, nc) * nc + wrap(ii - 3, nc)) * nc + wrap(kk - 3, nc);
+        const long long c = ((long long)wrap(jj - f.yhost, f.nyw) * nc + wrap(ii - 3, nc)) * nc + wrap(kk - 3, nc);
 #pragma unroll
         for (int q = 0; q < 5; ++q) stage[q * Nt + p] = f.W[q][c];
     }
@@ -729,7 +732,8 @@ __global__ void k_maxwave(FieldDev f, unsigned long long *out)
 {
     double m = 0.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
+    const long long plane = (long long)f.nc * f.nc, c1 = f.yhi * plane;
+    for (long long c = f.ylo * plane + (long long)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += stride) {
         const double den = f.W[0][c];
         const double u = __ddiv_rn(f.W[1][c], den), v = __ddiv_rn(f.W[2][c], den), w = __ddiv_rn(f.W[3][c], den);
         const double vsq = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
@@ -794,7 +798,9 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
     using ST = SplineTiles<AXIS, B, LW>;
     constexpr int NCI = ST::NCI;
     extern __shared__ double smem[];
-    const int nc = f.nc, nt = nc + 6;
+    // nodes of a line: nc + 6 along x / z; along y ny + 2 yhost (the same for a
+    // periodic field; a slab's ny stored planes, its ghosts included)
+    const int nc = f.nc, nt = AXIS == 0 ? f.ny + 2 * f.yhost : nc + 6;
     const long long n = f.ncell;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int tsz = ST::tile(nt);
@@ -804,16 +810,17 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
         return AXIS == 2 ? smem[a * tsz + line * nt + node] : smem[a * tsz + node * (LW + 1) + line];
     };
     for (int p = threadIdx.x; p < nt; p += blockDim.x) {
-        cpv[p] = f.spl_cp[p];
-        invv[p] = f.spl_inv[p];
+        cpv[p] = AXIS == 0 ? f.spl_cpy[p] : f.spl_cp[p];
+        invv[p] = AXIS == 0 ? f.spl_invy[p] : f.spl_inv[p];
     }
     // the block's lines: y / x lines are (outer, k) with k in [k0, k0 + LW),
-    // outer = i (y lines) or j (x lines); z lines are l in [l0, l0 + LW), l = j nc + i
+    // outer = i (y lines) or j (x lines, interior planes); z lines are l in
+    // [l0, l0 + LW), l = j nc + i (interior planes)
     const int nkb = (nc + LW - 1) / LW;
     const long long set = blockIdx.x;
-    const int outer = AXIS == 2 ? 0 : int(set / nkb);
-    const int k0 = AXIS == 2 ? 0 : int(set - (long long)outer * nkb) * LW;
-    const long long l0 = AXIS == 2 ? set * LW : 0;
+    const int outer = AXIS == 2 ? 0 : (AXIS == 1 ? f.ylo : 0) + int(set / nkb);
+    const int k0 = AXIS == 2 ? 0 : int(set - (long long)(outer - (AXIS == 1 ? f.ylo : 0)) * nkb) * LW;
+    const long long l0 = AXIS == 2 ? (long long)f.ylo * nc + set * LW : 0;
     // cell of line `line` at position q (0 .. nc-1) along the axis
     auto cell = [&](int line, int q) -> long long {
         if (AXIS == 0) return ((long long)q * nc + outer) * nc + k0 + line;
@@ -821,7 +828,7 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
         return (l0 + line) * nc + q;
     };
     auto active = [&](int line) -> bool {
-        return AXIS == 2 ? l0 + line < (long long)nc * nc : k0 + line < nc;
+        return AXIS == 2 ? l0 + line < (long long)f.yhi * nc : k0 + line < nc;
     };
     // visit every (node, line) of the set: y / x, LW consecutive threads on
     // the LW lines of one node; z, warp w along the nodes of line w
@@ -836,9 +843,10 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
             }
         }
     };
-    // stage rho and the momenta (node p holds cell wrap(p - 3)), then velocities
+    // stage rho and the momenta (node p holds cell wrap(p - 3); along y plane
+    // wrap(p - yhost, nyw), a slab's plane p), then velocities
     each([&](int p, int line) {
-        const long long c = cell(line, wrap(p - 3, nc));
+        const long long c = cell(line, AXIS == 0 ? wrap(p - f.yhost, f.nyw) : wrap(p - 3, nc));
 #pragma unroll
         for (int a = 0; a < 4; ++a) cp_async8(&T(a, p, line), f.W[a] + c);
     });
@@ -852,7 +860,7 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
     });
     __syncthreads();
     if (active(w)) {
-        const double s = f.spl_s;
+        const double s = AXIS == 0 ? f.spl_sy : f.spl_s;
         const int p0 = lane * B;
 #pragma unroll 1
         for (int c0 = 0; c0 < 3; c0 += NCI) {
@@ -970,10 +978,10 @@ __global__ void __launch_bounds__(32 * LW, B <= 9 ? 2 : 1) k_spline_scan(FieldDe
         }
     }
     __syncthreads();
-    // slopes of nodes 3 .. nt-4 (cells 0 .. nc-1)
+    // slopes of nodes 3 .. nt-4 (the interior cells)
     each([&](int p, int line) {
         if (p >= 3 && p <= nt - 4) {
-            const long long c = cell(line, p - 3);
+            const long long c = cell(line, AXIS == 0 ? p - f.yhost : p - 3);
 #pragma unroll
             for (int a = 1; a < 4; ++a) scr[(3 + 3 * (a - 1) + AXIS) * n + c] = T(a, p, line);
         }
@@ -1022,23 +1030,30 @@ __device__ __forceinline__ void cell_prim(const FieldDev &f, long long c, double
     T = P * ri * f.iR;
 }
 
-// One pass over the cells: the means PrintStats forms (update.cpp:659-712)
-// and, for the rms of p, T and 1/rho (update.cpp:751-762), the first two
-// moments of x - K with K the value at cell 0 (shifted one-pass variance,
-// well conditioned because K lies inside the field's range).
-__global__ void k_sums1(FieldDev f, const double *scr, double *partial)
+// One pass over the interior cells: the means PrintStats forms
+// (update.cpp:659-712) and, for the rms of p, T and 1/rho (update.cpp:751-762),
+// the first two moments of x - K with K the value at the first interior cell
+// (shifted one-pass variance, well conditioned because K lies inside the
+// field's range); K goes to kout[0..2].
+__global__ void k_sums1(FieldDev f, const double *scr, double *partial, double *kout)
 {
     const long long n = f.ncell;
+    const long long plane = (long long)f.nc * f.nc, c0 = f.ylo * plane, c1 = f.yhi * plane;
     double acc[NSUM1];
 #pragma unroll
     for (int i = 0; i < NSUM1; ++i) acc[i] = 0.0;
     double Kp, Kt, Kv;
     {
         double den, u, v, w;
-        cell_prim(f, 0, den, Kv, u, v, w, Kp, Kt);
+        cell_prim(f, c0, den, Kv, u, v, w, Kp, Kt);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        kout[0] = Kp;
+        kout[1] = Kt;
+        kout[2] = Kv;
     }
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
+    for (long long c = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += stride) {
         double den, ri, u, v, w, P, T;
         cell_prim(f, c, den, ri, u, v, w, P, T);
         const double *g = scr + 3 * n;
@@ -1087,7 +1102,8 @@ __global__ void k_finalize(const double *partial, int nblocks, int nsum, double 
 __global__ void k_check(FieldDev f, int *err)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < f.ncell; c += stride) {
+    const long long plane = (long long)f.nc * f.nc, c1 = f.yhi * plane;
+    for (long long c = f.ylo * plane + (long long)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += stride) {
         double w[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) w[q] = f.W[q][c];
@@ -1245,7 +1261,7 @@ cudaError_t launch_gather(const FieldDev &f, const double *stage, int nsm, cudaS
 cudaError_t launch_scatter(const FieldDev &f, double *stage, int nsm, cudaStream_t st, long long lo, long long hi)
 {
     const long long nt = f.nc + 6;
-    if (hi < 0) hi = nt * nt * nt;
+    if (hi < 0) hi = (f.ny + 2 * f.yhost) * nt * nt;
     if (hi <= lo) return cudaSuccess;
     k_scatter<<<helper_grid(hi - lo, 256, nsm), 256, 0, st>>>(f, stage, lo, hi);
     return cudaGetLastError();
@@ -1264,8 +1280,10 @@ cudaError_t spline_go(const FieldDev &f, double *scratch, cudaStream_t st)
     cudaError_t e = cudaFuncSetAttribute(k_spline_scan<AXIS, B, LW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)bytes);
     if (e != cudaSuccess) return e;
-    const long long sets = AXIS == 2 ? ((long long)f.nc * f.nc + LW - 1) / LW
-                                     : (long long)f.nc * ((f.nc + LW - 1) / LW);
+    // lines: y lines (i, k) of the whole slab, x and z lines of the interior planes
+    const long long ny = f.yhi - f.ylo;
+    const long long sets = AXIS == 2 ? (ny * f.nc + LW - 1) / LW
+                                     : (AXIS == 0 ? f.nc : ny) * ((f.nc + LW - 1) / LW);
     k_spline_scan<AXIS, B, LW><<<(unsigned)sets, 32 * LW, bytes, st>>>(f, scratch);
     return cudaGetLastError();
 }
@@ -1291,8 +1309,9 @@ cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, do
     if (e == cudaSuccess) e = spline_axis<1>(f, scratch, st);
     if (e == cudaSuccess) e = spline_axis<2>(f, scratch, st);
     if (e != cudaSuccess) return e;
-    k_sums1<<<grid, block, 0, st>>>(f, scratch, partial);
-    k_finalize<<<1, 32 * NSUM1, 0, st>>>(partial, grid, NSUM1, 1.0 / double(f.ncell), sums);
+    k_sums1<<<grid, block, 0, st>>>(f, scratch, partial, sums + NSUM1);
+    const double cells = double(f.yhi - f.ylo) * f.nc * f.nc;
+    k_finalize<<<1, 32 * NSUM1, 0, st>>>(partial, grid, NSUM1, 1.0 / cells, sums);
     return cudaGetLastError();
 }
 

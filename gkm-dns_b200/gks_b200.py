@@ -95,7 +95,17 @@ SIGNATURES = {
     "gks_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gks_timestep_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_void_p, DP]),
+    "gks_create_slab": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Phys), ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gks_stats_part": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP]),
+    "gks_stats_reduce": (ctypes.c_int, [DP, ctypes.c_int, ctypes.POINTER(Phys), ctypes.POINTER(StatsOut)]),
+    "gks_halo_buffers": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(ctypes.c_size_t)]),
+    "gks_halo_pack": (ctypes.c_int, [ctypes.c_void_p]),
+    "gks_halo_unpack": (ctypes.c_int, [ctypes.c_void_p]),
 }
+
+STATS_PART = 28  # doubles of one gks_stats_part record
 
 STAGES = ["recon_x", "flux_x", "recon_y", "flux_y", "recon_z", "flux_z", "update"]
 
@@ -148,25 +158,48 @@ def _ptrs(W: np.ndarray) -> DP5:
 @dataclasses.dataclass
 class _Field:
     nc: int
+    nty: int  # planes of the padded host block along y: nc + 6, or a slab's ny + 6
+
+
+def stats_reduce(parts: np.ndarray, phys: Phys) -> dict:
+    """Merge gks_stats_part records (one row of STATS_PART per part, e.g. per
+    rank) into the diagnostics of the whole field (gks_stats_reduce)."""
+    parts = np.ascontiguousarray(parts, dtype=np.float64).reshape(-1, STATS_PART)
+    out = StatsOut()
+    rc = load_library().gks_stats_reduce(parts.ctypes.data_as(DP), len(parts), ctypes.byref(phys), ctypes.byref(out))
+    if rc != 0:
+        raise GksError(rc, "gks_stats_reduce: bad parts")
+    return dict(zip(STATS_FIELDS, out.as_array()))
 
 
 class Solver:
-    """One context on the current CUDA device holding one or more fields."""
+    """One context on the current CUDA device holding one or more fields, or
+    (slab=(ny, y0)) the y-slab of ny interior planes from global plane y0 of
+    one field split over ranks (gks_create_slab)."""
 
-    def __init__(self, phys, precision: int = FP64, flags: int = 0, device: int | None = None):
+    def __init__(self, phys, precision: int = FP64, flags: int = 0, device: int | None = None,
+                 slab: tuple | None = None):
         lib = load_library()
         if device is not None:
             select_device(device)
         if isinstance(phys, Phys):
             phys = [phys]
-        arr = (Phys * len(phys))(*phys)
         h = ctypes.c_void_p()
-        rc = lib.gks_create(ctypes.byref(h), len(phys), arr, precision, flags)
+        if slab is None:
+            arr = (Phys * len(phys))(*phys)
+            rc = lib.gks_create(ctypes.byref(h), len(phys), arr, precision, flags)
+        else:
+            if len(phys) != 1:
+                raise ValueError("a slab context holds one field")
+            rc = lib.gks_create_slab(ctypes.byref(h), ctypes.byref(phys[0]), int(slab[0]), int(slab[1]),
+                                     precision, flags)
         if rc != 0:
-            raise GksError(rc, "gks_create failed (no CUDA device, bad constants or out of memory)")
+            raise GksError(rc, "context creation failed (no CUDA device, bad constants or out of memory)")
         self._lib = lib
         self._h = h
-        self.fields = [_Field(p.nc) for p in phys]
+        self.phys = list(phys)
+        self.slab = slab
+        self.fields = [_Field(p.nc, (slab[0] if slab else p.nc) + 6) for p in phys]
         self.precision = precision
         self.flags = flags
 
@@ -193,29 +226,32 @@ class Solver:
         self.close()
 
     # state ---------------------------------------------------------------
-    def upload(self, W: np.ndarray, f: int = 0):
-        """W: (5, nt, nt, nt) float64 in the reference's padded layout."""
+    def host_shape(self, f: int = 0) -> tuple:
+        """Shape of field f's padded host block: (5, nt, nt, nt), or (5, ny + 6, nt, nt) for a slab."""
         nt = self.fields[f].nc + 6
-        if W.shape != (5, nt, nt, nt):
-            raise ValueError(f"expected shape {(5, nt, nt, nt)}, got {W.shape}")
+        return (5, self.fields[f].nty, nt, nt)
+
+    def upload(self, W: np.ndarray, f: int = 0):
+        """W: float64 padded block in the reference's layout (host_shape)."""
+        if W.shape != self.host_shape(f):
+            raise ValueError(f"expected shape {self.host_shape(f)}, got {W.shape}")
         W = np.ascontiguousarray(W, dtype=np.float64)
         self._ck(self._lib.gks_upload(self._h, f, _ptrs(W)))
 
     def download(self, f: int = 0, out: np.ndarray | None = None) -> np.ndarray:
-        nt = self.fields[f].nc + 6
         if out is None:
-            out = np.empty((5, nt, nt, nt))
+            out = np.empty(self.host_shape(f))
         self._ck(self._lib.gks_download(self._h, f, _ptrs(out)))
         return out
 
     def evolve(self, W: np.ndarray, nsteps: int = 1, f: int = 0) -> np.ndarray:
-        """The reference's per-step call on host memory: W (5, nt, nt, nt) is
+        """The reference's per-step call on host memory: W (host_shape) is
         uploaded, advanced nsteps steps and overwritten with the result (ghosts
         as the periodic image).  One field and one step overlap the copies with
         the step; pass W in pinned memory for full overlap."""
-        nt = self.fields[f].nc + 6
-        if W.shape != (5, nt, nt, nt) or W.dtype != np.float64 or not W.flags["C_CONTIGUOUS"]:
-            raise ValueError(f"expected a C-contiguous float64 array of shape {(5, nt, nt, nt)}")
+        shape = self.host_shape(f)
+        if W.shape != shape or W.dtype != np.float64 or not W.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"expected a C-contiguous float64 array of shape {shape}")
         self._ck(self._lib.gks_evolve(self._h, f, _ptrs(W), nsteps))
         return W
 
@@ -245,6 +281,27 @@ class Solver:
         out = StatsOut()
         self._ck(self._lib.gks_stats(self._h, f, ctypes.byref(out)))
         return out.as_array()
+
+    def stats_part(self, f: int = 0) -> np.ndarray:
+        """Mergeable diagnostics record of field f (gks_stats_part): STATS_PART doubles."""
+        out = np.empty(STATS_PART)
+        self._ck(self._lib.gks_stats_part(self._h, f, out.ctypes.data_as(DP)))
+        return out
+
+    # halo exchange of a slab ------------------------------------------------
+    def halo_buffers(self) -> tuple:
+        """Device addresses of the slab's halo buffers (send south, send north,
+        receive south, receive north) and their length in doubles."""
+        ptrs = (ctypes.c_void_p * 4)()
+        n = ctypes.c_size_t()
+        self._ck(self._lib.gks_halo_buffers(self._h, ptrs, ctypes.byref(n)))
+        return [ptrs[i] for i in range(4)], n.value
+
+    def halo_pack(self):
+        self._ck(self._lib.gks_halo_pack(self._h))
+
+    def halo_unpack(self):
+        self._ck(self._lib.gks_halo_unpack(self._h))
 
     def device_fields(self, f: int = 0):
         arr = DP5()

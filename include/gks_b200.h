@@ -10,6 +10,8 @@
  *   void timestep(ptype *W[5])                                weno/src/update.cpp:1057-1079
  *   void PrintStats(ptype *W[5], UBspline_3d_d *splinep[5])   weno/src/update.cpp:638-784
  *   void HaloTransfer(...) on one periodic rank               weno/src/update.cpp:894-1054
+ *   HaloTransfer's y exchange between ranks (send_HaloS/N)    weno/src/update.cpp:899-954
+ *   segment() / procDim y-decomposition                       weno/src/FlowField.cpp:278-288, Main.cpp:21-30
  * The compatibility shim with the reference's own evolve()/DevAlloc
  * signatures is gkm-dns_b200/driver/gks_compat.h.
  *
@@ -148,6 +150,53 @@ int gks_step(gks_ctx *ctx, int nsteps);
 /* Diagnostics of field f on the current state (synchronises). */
 int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out);
 
+/* The diagnostics as a mergeable part, for a field split over ranks: part[28]
+ * receives the means over field f's interior cells of the 18 quantities
+ * PrintStats sums (update.cpp:659-712), the means of x - K and (x - K)^2 for
+ * x = p, T, 1/rho, the shifts K (x at the first interior cell) and the number
+ * of interior cells.  gks_stats_reduce merges the parts of all ranks (the
+ * reference's MPI_Reduce / MPI_Allreduce of the sums, update.cpp:714-762) into
+ * the normalised output; gks_stats(ctx, f, out) equals gks_stats_part followed
+ * by gks_stats_reduce of that one part. */
+int gks_stats_part(gks_ctx *ctx, int f, double *part);
+int gks_stats_reduce(const double *parts, int nparts, const gks_phys *phys, gks_stats_out *out);
+
+/* One y-slab of a periodic nc^3 field split over ranks along y -- the
+ * reference's decomposition with procDim = {P, 1, 1} (Main.cpp:21-30,
+ * segment(), FlowField.cpp:278-288): ny interior planes (nc_segy, >= 3)
+ * starting at global plane y0 (sta[0]).  Host arrays are the rank's padded
+ * block, (ny + 6) x (nc + 6) x (nc + 6); the device stores the ny interior
+ * planes with the three ghost planes either side, and x / z stay periodic
+ * inside the slab.  gks_upload takes the ghost planes from the host block;
+ * gks_download writes the interior planes with their x / z ghosts and leaves
+ * the y ghost planes as they were uploaded, as the reference's evolve leaves
+ * ghosts until the next HaloTransfer.  After the upload and after every step
+ * the caller exchanges the y halo (gks_halo_*), as the reference's Evolve
+ * calls HaloTransfer (update.cpp:106-108, 140-142): a step, and the
+ * diagnostics, read ghost planes that must hold the neighbours' current
+ * state.  gks_timestep gives the slab's own dt (the field's is the minimum
+ * over ranks); gks_stats_part its part of the diagnostics, with y-derivatives
+ * from splines over the slab's padded block as the reference's multi-rank
+ * PrintStats takes them (Interpolation.cpp:10-27).
+ * The stage timer and the tuner run whole-field launches and refuse a slab;
+ * gks_set_launch pins a configuration tuned on a periodic field. */
+int gks_create_slab(gks_ctx **out, const gks_phys *phys, int ny, int y0, int precision, int flags);
+
+/* The slab's four halo buffers in device memory, each 15 nc^2 doubles laid out
+ * [component][plane 0..2][nc^2] (send_HaloS / recv_HaloS of update.cpp:899-954
+ * without the x / z ghost columns): bufs[0] send south (interior planes 0-2),
+ * bufs[1] send north (the last three interior planes), bufs[2] receive from
+ * the south neighbour (its last three), bufs[3] receive from the north
+ * neighbour (its first three).  *elems (may be NULL) = 15 nc^2. */
+int gks_halo_buffers(gks_ctx *ctx, double **bufs, size_t *elems);
+
+/* Copy the boundary planes into the send buffers / the receive buffers into
+ * the ghost planes; asynchronous on the context's stream, like gks_step.
+ * One exchange step of the halo is pack, send south and north / receive from
+ * north and south (NCCL, MPI or a device copy), unpack. */
+int gks_halo_pack(gks_ctx *ctx);
+int gks_halo_unpack(gks_ctx *ctx);
+
 /* Wait for all work of the context. */
 int gks_sync(gks_ctx *ctx);
 
@@ -155,8 +204,9 @@ int gks_sync(gks_ctx *ctx);
  * GKS_ENONFINITE and names the first offending field in gks_last_error. */
 int gks_check(gks_ctx *ctx);
 
-/* Device-resident interior arrays of field f (nc^3 doubles each, index
- * (j*nc + i)*nc + k), for callers that keep the state on the GPU. */
+/* Device-resident arrays of field f (nc^3 doubles each, index
+ * (j*nc + i)*nc + k; for a slab (ny + 6) nc^2, its ghost planes included),
+ * for callers that keep the state on the GPU. */
 int gks_device_fields(gks_ctx *ctx, int f, double *dW[5]);
 
 /* Run subsequent work on a caller-provided cudaStream_t (NULL: the context's

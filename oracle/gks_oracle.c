@@ -558,23 +558,51 @@ static void line_slopes(long n, double h, const double *f, long stride, double *
     for (long i = n - 2; i >= 0; --i) m[i * stride] = dp[i] - cp[i] * m[(i + 1) * stride];
 }
 
-/* Slopes of field f (padded block) along axis 0 (j), 1 (i) or 2 (k). */
-static void axis_slopes(const double *f, double *g, long nt, double h, int axis, double *cp, double *dp)
+/* Slopes of field f (padded block of nty x nt x nt cells) along axis 0 (j), 1 (i) or 2 (k). */
+static void axis_slopes(const double *f, double *g, long nty, long nt, double h, int axis, double *cp, double *dp)
 {
     const long sj = nt * nt, si = nt;
-    for (long a = 0; a < nt; ++a)
+    const long na = axis == 0 ? nt : nty, len = axis == 0 ? nty : nt;
+    for (long a = 0; a < na; ++a)
         for (long b = 0; b < nt; ++b) {
             long base, stride;
             if (axis == 0) { base = a * si + b; stride = sj; }
             else if (axis == 1) { base = a * sj + b; stride = si; }
             else { base = a * sj + b * si; stride = 1; }
-            line_slopes(nt, h, f + base, stride, g + base, cp, dp);
+            line_slopes(len, h, f + base, stride, g + base, cp, dp);
         }
 }
 
-void orc_stats(const double *W, const orc_params *p, double *out)
+/* Spacing of a spline grid of num nodes from (sta - 3) dx + dx/2
+ * (Interpolation.cpp:10-27), as einspline derives it from start and end. */
+static double grid_h(long sta, long num, double dx)
 {
-    const long nc = p->nc, nt = nc + 6, N = nt * nt * nt;
+    const double start = (sta - 3) * dx + 0.5 * dx;
+    const double end = start + (num - 1) * dx;
+    return (end - start) / (double)(num - 1);
+}
+
+static void prim_at(const double *W, long cs, long c, double gam, double R, double *deni, double *ui,
+                    double *vi, double *wi, double *Vsqr, double *Pi, double *Ti)
+{
+    *deni = W[c];
+    *ui = W[cs + c] / *deni;
+    *vi = W[2 * cs + c] / *deni;
+    *wi = W[3 * cs + c] / *deni;
+    *Vsqr = (*ui * *ui + *vi * *vi + *wi * *wi);
+    *Pi = (*deni * (gam - 1)) * (W[4 * cs + c] / *deni - 0.5 * *Vsqr);
+    *Ti = *Pi / (R * *deni);
+}
+
+/* One rank's first pass of PrintStats (update.cpp:659-712) over its segment:
+ * W is its padded block of nty x nt x nt cells (components cs apart), its
+ * first plane the global plane sta0 - 3; the splines run over the segment's
+ * own nodes (einspline per rank, Interpolation.cpp:3-31).  Adds the 18 local
+ * sums to acc: TKE, Diss, SijSij, DUDX2-4, DVDY2-4, DWDZ2-4, P, T, 1/rho,
+ * |u|^2, c, rho. */
+static void seg_sums(const double *W, long cs, long nty, long nt, long sta0, const orc_params *p, double *acc)
+{
+    const long N = nty * nt * nt;
     const double gam = p->gam, R = p->R, dx = p->dx;
     double *u = malloc(sizeof(double) * N), *v = malloc(sizeof(double) * N), *w = malloc(sizeof(double) * N);
     double *gu[3], *gv[3], *gw[3];
@@ -583,90 +611,103 @@ void orc_stats(const double *W, const orc_params *p, double *out)
         gv[d] = malloc(sizeof(double) * N);
         gw[d] = malloc(sizeof(double) * N);
     }
-    double *cp = malloc(sizeof(double) * nt), *dp = malloc(sizeof(double) * nt);
+    const long nmax = nty > nt ? nty : nt;
+    double *cp = malloc(sizeof(double) * nmax), *dp = malloc(sizeof(double) * nmax);
     for (long c = 0; c < N; ++c) { /* generateSplines, update.cpp:1215-1224 */
         const double d = W[c];
-        u[c] = W[N + c] / d;
-        v[c] = W[2 * N + c] / d;
-        w[c] = W[3 * N + c] / d;
+        u[c] = W[cs + c] / d;
+        v[c] = W[2 * cs + c] / d;
+        w[c] = W[3 * cs + c] / d;
     }
-    /* grid of the spline (Interpolation.cpp:10-27), spacing as einspline derives it */
-    const double start = (0 - 3) * dx + 0.5 * dx;
-    const double end = start + (nt - 1) * dx;
-    const double h = (end - start) / (double)(nt - 1);
     for (int d = 0; d < 3; ++d) {
-        axis_slopes(u, gu[d], nt, h, d, cp, dp);
-        axis_slopes(v, gv[d], nt, h, d, cp, dp);
-        axis_slopes(w, gw[d], nt, h, d, cp, dp);
+        const double h = d == 0 ? grid_h(sta0, nty, dx) : grid_h(0, nt, dx);
+        axis_slopes(u, gu[d], nty, nt, h, d, cp, dp);
+        axis_slopes(v, gv[d], nty, nt, h, d, cp, dp);
+        axis_slopes(w, gw[d], nty, nt, h, d, cp, dp);
     }
-
-    double sTKE = 0, sDiss = 0, sSij = 0, u2 = 0, u3 = 0, u4 = 0, v2 = 0, v3 = 0, v4 = 0, w2 = 0, w3 = 0, w4 = 0;
-    double Pm = 0, Tm = 0, Vm = 0, q2 = 0, cm = 0, dm = 0;
-    for (long j = 3; j < nt - 3; ++j)
+    for (long j = 3; j < nty - 3; ++j)
         for (long i = 3; i < nt - 3; ++i)
             for (long k = 3; k < nt - 3; ++k) {
                 const long c = (j * nt + i) * nt + k;
-                const double deni = W[c];
-                const double ui = W[N + c] / deni, vi = W[2 * N + c] / deni, wi = W[3 * N + c] / deni;
-                const double Vsqr = (ui * ui + vi * vi + wi * wi);
-                const double Pi = (deni * (gam - 1)) * (W[4 * N + c] / deni - 0.5 * Vsqr);
-                const double Ti = Pi / (R * deni);
-                Pm += Pi;
-                Tm += Ti;
-                Vm += 1 / deni;
+                double deni, ui, vi, wi, Vsqr, Pi, Ti;
+                prim_at(W, cs, c, gam, R, &deni, &ui, &vi, &wi, &Vsqr, &Pi, &Ti);
+                acc[12] += Pi;
+                acc[13] += Ti;
+                acc[14] += 1 / deni;
                 const double dudx = gu[1][c], dudy = gu[0][c], dudz = gu[2][c];
                 const double dvdx = gv[1][c], dvdy = gv[0][c], dvdz = gv[2][c];
                 const double dwdx = gw[1][c], dwdy = gw[0][c], dwdz = gw[2][c];
                 const double mu = viscosity(p, Ti);
-                sDiss += mu * (dudx * dudx + dudy * dudy + dudz * dudz + dvdx * dvdx + dvdy * dvdy +
-                               dvdz * dvdz + dwdx * dwdx + dwdy * dwdy + dwdz * dwdz);
-                sTKE += deni * (u[c] * u[c] + v[c] * v[c] + w[c] * w[c]);
-                sSij += (dudx * dudx + 0.5 * ((dudy + dvdx) * (dudy + dvdx)) +
-                         0.5 * ((dudz + dwdx) * (dudz + dwdx)) + 0.5 * ((dwdy + dvdz) * (dwdy + dvdz)) +
-                         dvdy * dvdy + dwdz * dwdz);
-                u2 += dudx * dudx; u3 += dudx * dudx * dudx; u4 += dudx * dudx * dudx * dudx;
-                v2 += dvdy * dvdy; v3 += dvdy * dvdy * dvdy; v4 += dvdy * dvdy * dvdy * dvdy;
-                w2 += dwdz * dwdz; w3 += dwdz * dwdz * dwdz; w4 += dwdz * dwdz * dwdz * dwdz;
-                q2 += Vsqr;
-                cm += sqrt(gam * Pi / deni);
-                dm += deni;
+                acc[1] += mu * (dudx * dudx + dudy * dudy + dudz * dudz + dvdx * dvdx + dvdy * dvdy +
+                                dvdz * dvdz + dwdx * dwdx + dwdy * dwdy + dwdz * dwdz);
+                acc[0] += deni * (u[c] * u[c] + v[c] * v[c] + w[c] * w[c]);
+                acc[2] += (dudx * dudx + 0.5 * ((dudy + dvdx) * (dudy + dvdx)) +
+                           0.5 * ((dudz + dwdx) * (dudz + dwdx)) + 0.5 * ((dwdy + dvdz) * (dwdy + dvdz)) +
+                           dvdy * dvdy + dwdz * dwdz);
+                acc[3] += dudx * dudx; acc[4] += dudx * dudx * dudx; acc[5] += dudx * dudx * dudx * dudx;
+                acc[6] += dvdy * dvdy; acc[7] += dvdy * dvdy * dvdy; acc[8] += dvdy * dvdy * dvdy * dvdy;
+                acc[9] += dwdz * dwdz; acc[10] += dwdz * dwdz * dwdz; acc[11] += dwdz * dwdz * dwdz * dwdz;
+                acc[15] += Vsqr;
+                acc[16] += sqrt(gam * Pi / deni);
+                acc[17] += deni;
             }
-    const double Nc = (double)(nc * nc * nc);
-    sTKE /= Nc; sDiss /= Nc; sSij /= Nc;
-    u2 /= Nc; u3 /= Nc; u4 /= Nc; v2 /= Nc; v3 /= Nc; v4 /= Nc; w2 /= Nc; w3 /= Nc; w4 /= Nc;
-    Pm /= Nc; Tm /= Nc; Vm /= Nc;
-    double Pr = 0, Tr = 0, Vr = 0;
-    for (long j = 3; j < nt - 3; ++j)
-        for (long i = 3; i < nt - 3; ++i)
-            for (long k = 3; k < nt - 3; ++k) {
-                const long c = (j * nt + i) * nt + k;
-                const double deni = W[c];
-                const double ui = W[N + c] / deni, vi = W[2 * N + c] / deni, wi = W[3 * N + c] / deni;
-                const double Vsqr = (ui * ui + vi * vi + wi * wi);
-                const double Pi = (deni * (gam - 1)) * (W[4 * N + c] / deni - 0.5 * Vsqr);
-                const double Ti = Pi / (R * deni);
-                Pr += (Pm - Pi) * (Pm - Pi);
-                Tr += (Tm - Ti) * (Tm - Ti);
-                Vr += (Vm - 1 / deni) * (Vm - 1 / deni);
-            }
-    Pr = sqrt(Pr / Nc);
-    Tr = sqrt(Tr / Nc);
-    Vr = sqrt(Vr / Nc);
-    out[0] = sTKE;
-    out[1] = sDiss;
-    out[2] = u3 / pow(u2, 1.5);
-    out[3] = v3 / pow(v2, 1.5);
-    out[4] = w3 / pow(w2, 1.5);
-    out[5] = u4 / (u2 * u2);
-    out[6] = v4 / (v2 * v2);
-    out[7] = w4 / (w2 * w2);
-    out[8] = Pr / (gam * p->p0 * p->Mt * p->Mt);
-    out[9] = Tr / ((gam - 1) * p->T0 * p->Mt * p->Mt);
-    out[10] = Vr / (p->Mt * p->Mt / p->den0);
-    out[11] = sSij;
-    out[12] = sqrt(q2 / Nc) / (cm / Nc);
-    out[13] = dm / Nc;
     free(u); free(v); free(w);
     for (int d = 0; d < 3; ++d) { free(gu[d]); free(gv[d]); free(gw[d]); }
     free(cp); free(dp);
 }
+
+/* One rank's second pass (update.cpp:751-757): squared deviations from the
+ * global means m[0..2] of p, T and 1/rho over its segment's interior. */
+static void seg_devs(const double *W, long cs, long nty, long nt, const orc_params *p, const double *m, double *acc)
+{
+    for (long j = 3; j < nty - 3; ++j)
+        for (long i = 3; i < nt - 3; ++i)
+            for (long k = 3; k < nt - 3; ++k) {
+                const long c = (j * nt + i) * nt + k;
+                double deni, ui, vi, wi, Vsqr, Pi, Ti;
+                prim_at(W, cs, c, p->gam, p->R, &deni, &ui, &vi, &wi, &Vsqr, &Pi, &Ti);
+                acc[0] += (m[0] - Pi) * (m[0] - Pi);
+                acc[1] += (m[1] - Ti) * (m[1] - Ti);
+                acc[2] += (m[2] - 1 / deni) * (m[2] - 1 / deni);
+            }
+}
+
+void orc_stats_ranks(const double *W, const orc_params *p, int nranks, double *out)
+{
+    const long nc = p->nc, nt = nc + 6, cs = nt * nt * nt, ny = nc / nranks, nty = ny + 6;
+    const double gam = p->gam;
+    /* every rank's segment is planes [r ny, r ny + ny + 6) of the padded block
+     * (segment() / segmentFill, FlowField.cpp:278-303); its sums reduced in
+     * rank order (MPI_Reduce, update.cpp:714-725) */
+    double s[18] = {0};
+    for (int r = 0; r < nranks; ++r) {
+        double acc[18] = {0};
+        seg_sums(W + r * ny * nt * nt, cs, nty, nt, r * ny, p, acc);
+        for (int i = 0; i < 18; ++i) s[i] += acc[i];
+    }
+    const double Nc = (double)(nc * nc * nc);
+    for (int i = 0; i < 18; ++i) s[i] /= Nc;
+    double dv[3] = {0, 0, 0};
+    for (int r = 0; r < nranks; ++r) {
+        double acc[3] = {0, 0, 0};
+        seg_devs(W + r * ny * nt * nt, cs, nty, nt, p, s + 12, acc);
+        for (int i = 0; i < 3; ++i) dv[i] += acc[i];
+    }
+    const double Pr = sqrt(dv[0] / Nc), Tr = sqrt(dv[1] / Nc), Vr = sqrt(dv[2] / Nc);
+    out[0] = s[0];
+    out[1] = s[1];
+    out[2] = s[4] / pow(s[3], 1.5);
+    out[3] = s[7] / pow(s[6], 1.5);
+    out[4] = s[10] / pow(s[9], 1.5);
+    out[5] = s[5] / (s[3] * s[3]);
+    out[6] = s[8] / (s[6] * s[6]);
+    out[7] = s[11] / (s[9] * s[9]);
+    out[8] = Pr / (gam * p->p0 * p->Mt * p->Mt);
+    out[9] = Tr / ((gam - 1) * p->T0 * p->Mt * p->Mt);
+    out[10] = Vr / (p->Mt * p->Mt / p->den0);
+    out[11] = s[2];
+    out[12] = sqrt(s[15]) / s[16];
+    out[13] = s[17];
+}
+
+void orc_stats(const double *W, const orc_params *p, double *out) { orc_stats_ranks(W, p, 1, out); }

@@ -74,6 +74,12 @@ double orc_maxval(const double *W, const orc_params *p);
  * SijSij, Mt (sqrt<|u|^2> / <c>), mean density. */
 void orc_stats(const double *W, const orc_params *p, double *out);
 
+/* The same for the field split over nranks ranks along y (procDim = {nranks,
+ * 1, 1}; nc divisible by nranks): every rank's sums over its own segment,
+ * with splines over the segment's padded nodes, reduced over the ranks as the
+ * reference's PrintStats does with MPI (update.cpp:638-784). */
+void orc_stats_ranks(const double *W, const orc_params *p, int nranks, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,7 @@ def lib():
         L.orc_maxval.argtypes = [dp, ctypes.POINTER(OrcParams)]
         L.orc_maxval.restype = ctypes.c_double
         L.orc_stats.argtypes = [dp, ctypes.POINTER(OrcParams), dp]
+        L.orc_stats_ranks.argtypes = [dp, ctypes.POINTER(OrcParams), ctypes.c_int, dp]
         _lib = L
     return _lib
 
@@ -124,6 +125,13 @@ def maxval(W: np.ndarray, prm: OrcParams) -> float:
 def stats(W: np.ndarray, prm: OrcParams) -> np.ndarray:
     out = np.empty(14)
     lib().orc_stats(_p(np.ascontiguousarray(W)), ctypes.byref(prm), _p(out))
+    return out
+
+
+def stats_ranks(W: np.ndarray, prm: OrcParams, nranks: int) -> np.ndarray:
+    """Diagnostics of the field split over nranks ranks along y (orc_stats_ranks)."""
+    out = np.empty(14)
+    lib().orc_stats_ranks(_p(np.ascontiguousarray(W)), ctypes.byref(prm), nranks, _p(out))
     return out
 
 
