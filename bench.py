@@ -677,6 +677,101 @@ def run_ours(args):
     return 0
 
 
+def run_slabs(args):
+    """One nc^3 field split over the ranks along y (gks_slabs: NCCL halo
+    exchange after every step), or with --local-slabs P over P slabs in this
+    process on one GPU (device-copy exchange): strong scaling of one field,
+    the halo exchange inside the timed steps.  Not the headline line."""
+    import socket
+
+    import torch
+    import torch.distributed as tdist
+
+    import gks_b200 as gks
+    import gks_ic
+    import gks_slabs
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    gks.select_device(local)
+    local_p = args.local_slabs
+    if not local_p and not tdist.is_initialized():
+        import datetime
+
+        if ws == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            if "MASTER_PORT" not in os.environ:
+                with socket.socket() as sk:
+                    sk.bind(("127.0.0.1", 0))
+                    os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+    nc = args.nc
+    case = make_case(nc, 0, args.mach, args.re)
+    W = gks_ic.to_conservative_padded(case)
+    phys = gks.phys_from_case(case)
+    tuned = None
+    if not args.no_tune:
+        with gks.Solver(phys, gks.FP64, device=local) as s:
+            s.upload(W)
+            s.timestep(CFL)
+            s.autotune(2)
+            tuned = s.launch_config()
+    if local_p:
+        f = gks_slabs.LocalSlabs(phys, local_p, gks.FP64)
+        solvers, nslabs = f.solvers, local_p
+        f.upload(W)
+    else:
+        f = gks_slabs.SlabField(phys, gks.FP64)
+        solvers, nslabs = [f.solver], ws
+        f.upload(gks_slabs.split_block(W, ws, rank))
+    del W
+    if tuned:
+        for s in solvers:
+            for kind in ("recon", "flux"):
+                for d, a in enumerate("xyz"):
+                    c = tuned[f"{kind}_{a}"]
+                    s.set_launch(kind, d, c["variant"], c["grid"])
+    dt = f.timestep(CFL)
+    f.step(args.warmup)
+    f.sync()
+    if not local_p:
+        tdist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(f.stream)
+    f.step(args.steps)
+    e1.record(f.stream)
+    e1.synchronize()
+    f.sync()
+    ms = e0.elapsed_time(e1) / args.steps
+    if not local_p and ws > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = f.stats()
+    f.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": nc ** 3 / (ms * 1e-3), "unit": UNIT, "n_gpus": 1 if local_p else ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": f"synthetic: seeded solenoidal DHIT field (k0 {K0}, Mt {args.mach:g}, Re_lambda {args.re:g})",
+                "config": {"workload": f"DHIT {nc}^3 WENO-GKS step, FP64, one field in {nslabs} y-slabs",
+                           "nc": nc, "slabs": nslabs, "slab_planes": nc // nslabs,
+                           "exchange": "device copy, one process" if local_p else "NCCL send/recv, one rank per GPU",
+                           "parallelism": f"y-slabs x{nslabs}", "tuned": bool(tuned)},
+                "dt": dt, "stats": {k: float(v) for k, v in st.items()},
+                "e2e": None, "e2e_note": "device-resident slabs; the host per-step call is the default line's"}
+        print(json.dumps(line), flush=True)
+    if not local_p:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -695,6 +790,10 @@ def main():
                     help="with --accuracy: compare FP64 with FP64 started from the initial field rounded to FP32")
     ap.add_argument("--mach", type=float, default=MACH, help="turbulent Mach number of the field")
     ap.add_argument("--re", type=float, default=RE, help="Re_lambda of the field")
+    ap.add_argument("--slabs", action="store_true",
+                    help="one field split over the ranks along y (NCCL halo exchange); strong scaling")
+    ap.add_argument("--local-slabs", type=int, default=0,
+                    help="one field split into this many y-slabs in one process on one GPU")
     args = ap.parse_args()
     if args.accuracy:
         return run_accuracy(args)
@@ -702,6 +801,8 @@ def main():
         ap.error("at least 3 warm-up steps")
     if args.impl == "reference":
         return run_reference(args)
+    if args.slabs or args.local_slabs:
+        return run_slabs(args)
     return run_ours(args)
 
 

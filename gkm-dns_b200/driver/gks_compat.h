@@ -9,8 +9,11 @@
 // -DUseGPU and link -lgks_b200.  The call site in update.cpp stays unchanged.
 //
 // Semantics: one periodic block per process (procDim 1x1x1; the kernels wrap
-// the halo themselves, so a multi-rank decomposition is refused), FP64 by
-// default.  Compile-time options:
+// the halo themselves), or one y-slab per rank of a field split along y
+// (procDim = {P, 1, 1}: a gks_create_slab context of nc_segy planes from
+// sta[0], whose y ghosts come from the caller's HaloTransfer as in the
+// reference); decompositions along x or z are refused.  FP64 by default.
+// Compile-time options:
 //   GKS_COMPAT_MIXED          use the mixed FP32/FP64 path
 //   GKS_COMPAT_GPU_SEMANTICS  reproduce the reference GPU kernel's choices
 //                             (WENO on rho E, no 1/Pr factor) instead of the
@@ -21,10 +24,11 @@
 //                             and ~DevAlloc releases them; the reference
 //                             allocates W once per run, Main.cpp:36)
 // As in the reference, evolve() uploads W, advances one step and downloads W
-// (gks_evolve: the copies overlap the step slab by slab; with W in pinned host
-// memory both PCIe directions and the step run concurrently); the downloaded
-// ghosts already hold the periodic image, so the caller's HaloTransfer that
-// follows leaves them unchanged.
+// (gks_evolve: for a whole periodic block the copies overlap the step slab by
+// slab; with W in pinned host memory both PCIe directions and the step run
+// concurrently); the downloaded x / z ghosts, and a whole block's y ghosts,
+// already hold the periodic image, and the caller's HaloTransfer that follows
+// refreshes a slab's y ghosts from its neighbours.
 #pragma once
 
 #include <cstdio>
@@ -95,8 +99,11 @@ inline void gks_compat_check(gks_ctx *ctx, int rc, const char *what)
 
 inline DevAlloc::DevAlloc()
 {
-    if (procDim[0] * procDim[1] * procDim[2] != 1 || nc_segx != nc_segy || nc_segx != nc_segz) {
-        fprintf(stderr, "gks_b200: one periodic cube per process is required (procDim 1x1x1)\n");
+    // procDim[0] splits y (FlowField.cpp:22, segment() :282)
+    const bool whole = procDim[0] == 1 && nc_segy == nc_segx;
+    if (procDim[1] != 1 || procDim[2] != 1 || nc_segx != nc_segz || nc_segy * procDim[0] != nc_segx) {
+        fprintf(stderr, "gks_b200: one periodic cube per process or a split along y only (procDim {P,1,1}) "
+                        "is required\n");
         abort();
     }
     gks_phys p{};
@@ -124,7 +131,8 @@ inline DevAlloc::DevAlloc()
 #else
     const int precision = GKS_FP64;
 #endif
-    gks_compat_check(nullptr, gks_create(&ctx, 1, &p, precision, flags), "gks_create");
+    if (whole) gks_compat_check(nullptr, gks_create(&ctx, 1, &p, precision, flags), "gks_create");
+    else gks_compat_check(nullptr, gks_create_slab(&ctx, &p, nc_segy, sta[0], precision, flags), "gks_create_slab");
 }
 
 inline void evolve(ptype *W[5], DevAlloc *dev, ptype dt)

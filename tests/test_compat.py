@@ -61,6 +61,38 @@ def test_compat_evolve_matches_solver(tmp_path, gks):
 
 
 @pytest.mark.gpu
+def test_compat_evolve_on_y_split_ranks(tmp_path, gks):
+    """The shim under the reference's y decomposition (procDim = {2, 1, 1}):
+    each rank's evolve(W, dev, dt) advances its slab block, whose y ghosts the
+    caller's HaloTransfer refreshes between steps (here: merged and split
+    again on the host); two steps equal the whole field's."""
+    import gks_slabs
+
+    case = gks_ic.make_dhit(16, k0=4.0, Mt=0.3, seed=6)
+    W = gks_ic.to_conservative_padded(case)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W)
+        dt = s.timestep(0.5)
+        s.step(2)
+        s.sync()
+        ref = s.download()
+    exe = str(tmp_path / "compat_main")
+    build_compat(exe)
+    cur = W
+    for step in range(2):
+        blocks = []
+        for r in range(2):
+            b = gks_slabs.split_block(cur, 2, r)
+            b.tofile(str(tmp_path / "in.bin"))
+            subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), "16", repr(dt), "1",
+                            repr(case.gam), repr(case.mu0), repr(case.p0), "1.0", repr(case.Mt), repr(case.t0),
+                            "2", str(r)], check=True)
+            blocks.append(np.fromfile(str(tmp_path / "out.bin")).reshape(b.shape))
+        cur = gks_slabs.merge_blocks(blocks)  # HaloTransfer
+    assert np.array_equal(cur, ref)
+
+
+@pytest.mark.gpu
 def test_driver_prints_reference_lines(tmp_path, oracle):
     """gks_dns on the 16^3 golden case prints the reference's statistics lines."""
     g = np.load(os.path.join(ROOT, "tests", "golden", "dhit16.npz"))
