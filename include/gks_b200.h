@@ -258,12 +258,13 @@ int gks_peak_flops(int precision, double *tflops);
  * Returns dt = cfl * (2 pi/nc) / max(|u| + c) in *dt_out (host memory), the
  * same value gks_timestep gives; it synchronises `stream` (NULL: the legacy
  * default stream) to hand dt back.  Limit: nc <= 1024, else GKS_ETOOBIG.
- * Scratch is a fixed file-scope device array of 1026 64-bit words that every
- * GPU loading the library holds until exit; the first call on a device (and
- * the first after its CUDA context is replaced, e.g. by cudaDeviceReset)
- * looks up the array's address, so make that first call before any stream
- * capture.  Calls share the scratch: calls that overlap on the GPU race and
- * must be serialised. */
+ * It cannot be called while `stream` is being captured into a graph: it
+ * synchronises the stream and copies dt into host memory, neither of which a
+ * capture allows.  Scratch is a fixed file-scope device array of 1026 64-bit
+ * words that every GPU loading the library holds until exit; the first call
+ * on a device (and the first after its CUDA context is replaced, e.g. by
+ * cudaDeviceReset) looks up the array's address.  Calls share the scratch:
+ * calls that overlap on the GPU race and must be serialised. */
 int gks_timestep_noalloc(const double *const dW[5], int nc, double gam, double cfl, void *stream,
                          double *dt_out);
 
