@@ -1035,7 +1035,7 @@ __device__ __forceinline__ void cell_prim(const FieldDev &f, long long c, double
 // the first two moments of x - K with K the value at the first interior cell
 // (shifted one-pass variance, well conditioned because K lies inside the
 // field's range); K goes to kout[0..2].
-__global__ void k_sums1(FieldDev f, const double *scr, double *partial, double *kout)
+__global__ void __launch_bounds__(256, 2) k_sums1(FieldDev f, const double *scr, double *partial, double *kout)
 {
     const long long n = f.ncell;
     const long long plane = (long long)f.nc * f.nc, c0 = f.ylo * plane, c1 = f.yhi * plane;
