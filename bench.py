@@ -16,9 +16,12 @@ ours       K timed steps of the FP64 path (the parity path, `value`) and of the
            download) per step.  `roofline` is the dominant kernel (the flux
            sweep) timed live with CUDA events against the FP64 FMA peak
            measured live on the same GPU.  Under torchrun every rank advances
-           its own replica (replicas only: the path does not shard).
+           its own replica (replicas: the default line).
            The line also carries the mixed path's accuracy against the FP64
            path on the same field run to t/t0 = 2 (statistics every 10 steps).
+--slabs    one field split over the torchrun ranks along y (gks_slabs, NCCL
+           halo exchange after every step; strong scaling); --local-slabs P
+           runs P slabs of one field in one process on one GPU.
 reference  the reference's own CPU implementation (oracle/_ref, compiled from
            its sources) on the host cores: the 256^3 field cut into P y-slabs
            (P the largest power of two up to the core count, at most 64), one
@@ -601,6 +604,14 @@ def run_ours(args):
                      "frac": rate / (peak64 / 2),
                      "note": "FP64 instructions per second against the FP64 FMA instruction rate: "
                              "pipe utilisation (a DMUL or DADD occupies the pipe like a DFMA)"}
+        # the probe runs below the power cap, the step at it: the same fraction
+        # against the probe's rate scaled to the SM clock sampled in the timed
+        # FP64 steps (pipe utilisation per cycle, as ncu counts it)
+        probe_mhz = (peaks.get("probe_clocks") or {}).get("sm_mhz")
+        step_mhz = (results["fp64"]["clocks"] or {}).get("sm_mhz")
+        if probe_mhz and step_mhz:
+            fp64_pipe.update({"sm_mhz_probe": probe_mhz, "sm_mhz_step": step_mhz,
+                              "frac_clock_matched": rate / (peak64 / 2 * step_mhz / probe_mhz)})
     st64, st32 = results["fp64"]["stats"], results["mixed"]["stats"]
     rel = {k: abs(st32[k] - st64[k]) / abs(st64[k]) for k in ("tke", "diss", "skew_u", "skew_v", "skew_w")}
 
@@ -668,6 +679,7 @@ def run_ours(args):
             "mixed_over_fp64": mixed_value / value,
             "e2e_cell_updates_per_s": line["e2e"]["value"],
             "flux_fp64_pipe_frac": fp64_pipe["frac"] if fp64_pipe else None,
+            "flux_fp64_pipe_frac_clock_matched": fp64_pipe.get("frac_clock_matched") if fp64_pipe else None,
             "mixed_rel_err_t2_final": {k: acc["rel_err_final"][k] for k in ("tke", "diss")} if acc else None,
             "mixed_rel_err_t2_max": {k: acc["rel_err_max_over_history"][k] for k in ("tke", "diss")} if acc else None,
             "stats_ms": stats_ms,
