@@ -790,6 +790,8 @@ int gks_evolve(gks_ctx *ctx, int f, double *const W[5], int nsteps)
     for (int q = 0; q < 5; ++q)
         if (!W[q]) return fail(ctx, GKS_EINVAL, "null component pointer");
     if (nsteps < 1) return fail(ctx, GKS_EINVAL, "nsteps must be at least 1");
+    if (ctx->fh[f].slab && nsteps > 1)
+        return fail(ctx, GKS_EINVAL, "a slab advances one step per call: its ghosts come from the caller's halo exchange");
     if (!ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "evolve before dt of field " + std::to_string(f));
     CK(cudaSetDevice(ctx->device));
     if (ctx->nfields == 1 && nsteps == 1 && ctx->fh[f].phys.nc >= kPipeMinNc && !ctx->fh[f].slab)
@@ -862,6 +864,8 @@ int gks_step(gks_ctx *ctx, int nsteps)
 {
     if (!ctx) return GKS_EINVAL;
     if (nsteps < 0) return fail(ctx, GKS_EINVAL, "negative step count");
+    if (ctx->fh[0].slab && nsteps > 1)
+        return fail(ctx, GKS_EINVAL, "a slab advances one step between halo exchanges");
     for (int f = 0; f < ctx->nfields; ++f) {
         if (!ctx->fh[f].uploaded) return fail(ctx, GKS_ESTATE, "step before upload of field " + std::to_string(f));
         if (!ctx->fh[f].have_dt) return fail(ctx, GKS_ESTATE, "step before dt of field " + std::to_string(f));

@@ -178,8 +178,10 @@ int gks_stats_reduce(const double *parts, int nparts, const gks_phys *phys, gks_
  * over ranks); gks_stats_part its part of the diagnostics, with y-derivatives
  * from splines over the slab's padded block as the reference's multi-rank
  * PrintStats takes them (Interpolation.cpp:10-27).
- * The stage timer and the tuner run whole-field launches and refuse a slab;
- * gks_set_launch pins a configuration tuned on a periodic field. */
+ * gks_step and gks_evolve advance a slab one step per call (more return
+ * GKS_EINVAL: its ghosts would go stale).  The stage timer and the tuner run
+ * whole-field launches and refuse a slab; gks_set_launch pins a
+ * configuration tuned on a periodic field. */
 int gks_create_slab(gks_ctx **out, const gks_phys *phys, int ny, int y0, int precision, int flags);
 
 /* The slab's four halo buffers in device memory, each 15 nc^2 doubles laid out

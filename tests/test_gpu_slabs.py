@@ -130,6 +130,11 @@ def test_slab_rejects_whole_field_launches_and_bad_geometry(gks):
             s.autotune(1)
         s.step(1)
         s.sync()
+        # one step per call: more would read stale ghosts
+        with pytest.raises(gks.GksError):
+            s.step(2)
+        with pytest.raises(gks.GksError):
+            s.evolve(gks_slabs.split_block(W, 2, 1), nsteps=2)
     with gks.Solver(phys) as s:
         with pytest.raises(gks.GksError):
             s.halo_pack()
