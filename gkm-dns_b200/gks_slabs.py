@@ -82,6 +82,28 @@ def exchange_halo(bufs, rank: int, nranks: int, group=None):
         w.wait()
 
 
+def min_over_ranks(x: float, device, group=None) -> float:
+    """The smallest of every rank's x (the field's dt from the slabs' dts:
+    MPI_Allreduce of the maximum wave speed in the reference)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
+    return float(t.item())
+
+
+def gather_parts(part: np.ndarray, device, group=None) -> np.ndarray:
+    """Every rank's statistics part (gks_stats_part), in rank order, on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.from_numpy(np.ascontiguousarray(part, dtype=np.float64)).to(device)
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(parts, t, group=group)
+    return torch.stack(parts).cpu().numpy()
+
+
 class _DeviceArray:
     """A device allocation of the library as a 1-D float64 array for torch."""
 
@@ -143,12 +165,9 @@ class SlabField:
         """dt of the whole field: the minimum of the slabs' (update.cpp:1057-1079
         with the maximum wave speed taken over every rank)."""
         import torch
-        import torch.distributed as dist
 
         with torch.cuda.stream(self.stream):
-            t = torch.tensor([self.solver.timestep(cfl)], dtype=torch.float64, device=self.device)
-            dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
-            dt = float(t.item())
+            dt = min_over_ranks(self.solver.timestep(cfl), self.device, self.group)
         self.solver.set_dt(dt)
         return dt
 
@@ -164,14 +183,10 @@ class SlabField:
     def stats(self) -> dict:
         """The whole field's diagnostics on every rank (parts merged in rank order)."""
         import torch
-        import torch.distributed as dist
 
         with torch.cuda.stream(self.stream):
-            part = torch.from_numpy(self.solver.stats_part()).to(self.device)
-            parts = [torch.empty_like(part) for _ in range(self.nranks)]
-            dist.all_gather(parts, part, group=self.group)
-            merged = torch.stack(parts).cpu().numpy()
-        return gks.stats_reduce(merged, self.phys)
+            parts = gather_parts(self.solver.stats_part(), self.device, self.group)
+        return gks.stats_reduce(parts, self.phys)
 
 
 class LocalSlabs:

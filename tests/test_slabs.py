@@ -77,6 +77,42 @@ def test_halo_exchange_between_gloo_ranks(ws):
         assert u1 and u2
 
 
+def _reduce_rank(rank, ws, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", rank=rank, world_size=ws)
+    try:
+        dt = gks_slabs.min_over_ranks(1e-3 * (1 + 0.5 * ((rank + 1) % ws)), "cpu")
+        part = np.full(28, float(rank))
+        parts = gks_slabs.gather_parts(part, "cpu")
+        q.put((rank, dt, parts.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("ws", [2, 3])
+def test_dt_and_statistics_parts_over_gloo_ranks(ws):
+    """The slabs' dt is the minimum over ranks and every rank sees all ranks'
+    statistics parts in rank order (SlabField.timestep / SlabField.stats)."""
+    pytest.importorskip("torch")
+    import torch.multiprocessing as mp
+
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_reduce_rank, args=(r, ws, port, q)) for r in range(ws)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = sorted(q.get(timeout=10) for _ in range(ws))
+    for rank, dt, parts in got:
+        assert dt == 1e-3
+        assert [row[0] for row in parts] == [float(r) for r in range(ws)]
+
+
 def test_single_rank_exchange_is_a_local_copy():
     torch = pytest.importorskip("torch")
     bufs = [torch.full((4,), 1.0), torch.full((4,), 2.0), torch.zeros(4), torch.zeros(4)]
