@@ -259,7 +259,11 @@ int build_graph(gks_ctx *ctx)
 //
 // Planes are counted in an unwrapped y coordinate u in [-3, nc - 3) (plane
 // u mod nc), uploaded in increasing u: first the three planes below 0 (nc-3
-// .. nc-1), then slabs of about nc / kPipeSlabs planes.  With F the uploaded
+// .. nc-1), then thin slabs (4, 4, 8 planes), so that the first updated
+// planes start down early, slabs of about nc / kPipeSlabs planes, and thin
+// slabs again (8, 4, 4), so that little work is left after the last upload.
+// The y ghost planes go down with the planes they copy: the top ones
+// (images of planes 0-2) early, the bottom ones (nc-3 .. nc-1) last.  With F the uploaded
 // frontier, the stages advance as far as the planes they read allow (each
 // stage covers every plane once):
 //   x, z reconstruction  u in [-3, nc-3)   needs W(u)                    u < F
@@ -275,6 +279,31 @@ int build_graph(gks_ctx *ctx)
 // ---------------------------------------------------------------------------
 constexpr int kPipeSlabs = 24;
 constexpr int kPipeMinNc = 16;
+constexpr int kPipeEvents = kPipeSlabs + 16; // events per direction: at least the slabs + 1
+
+// The upload slabs of a field of nc planes, in unwrapped planes (see above).
+std::vector<std::pair<long long, long long>> pipe_slabs(long long nc)
+{
+    std::vector<std::pair<long long, long long>> s{{-3, 0}};
+    const long long n = nc - 3, S = (n + kPipeSlabs - 1) / kPipeSlabs;
+    const long long head[3] = {4, 4, 8}, tail[3] = {8, 4, 4};
+    long long a = 0;
+    if (n >= 32 + 2 * S) {
+        for (long long w : head) {
+            s.push_back({a, a + w});
+            a += w;
+        }
+        for (; a < n - 16; a += S) s.push_back({a, std::min(a + S, n - 16)});
+        a = n - 16;
+        for (long long w : tail) {
+            s.push_back({a, a + w});
+            a += w;
+        }
+        return s;
+    }
+    for (; a < n; a += S) s.push_back({a, std::min(a + S, n)});
+    return s;
+}
 
 int ensure_pipe(gks_ctx *ctx, FieldHost &h)
 {
@@ -297,12 +326,12 @@ int ensure_pipe(gks_ctx *ctx, FieldHost &h)
     }
     if (!ctx->h2d) CK(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
     if (!ctx->d2h) CK(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
-    while ((int)ctx->ev_in.size() < kPipeSlabs + 2) {
+    while ((int)ctx->ev_in.size() < kPipeEvents) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->ev_in.push_back(e);
     }
-    while ((int)ctx->ev_out.size() < kPipeSlabs + 2) {
+    while ((int)ctx->ev_out.size() < kPipeEvents) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->ev_out.push_back(e);
@@ -405,10 +434,9 @@ int evolve_slabs(gks_ctx *ctx, double *const W[5])
     const size_t pitch = (size_t)Nt * sizeof(double);
     bool contiguous = pitch <= (size_t)max_pitch;
     for (int q = 1; q < 5 && contiguous; ++q) contiguous = W[q] == W[0] + q * Nt;
-    // slabs in unwrapped planes: [-3, 0), then [(k-1) S, min(k S, nc-3))
-    const long long S = (nc - 3 + kPipeSlabs - 1) / kPipeSlabs;
-    std::vector<std::pair<long long, long long>> slabs{{-3, 0}};
-    for (long long a = 0; a < nc - 3; a += S) slabs.push_back({a, std::min(a + S, nc - 3)});
+    const std::vector<std::pair<long long, long long>> slabs = pipe_slabs(nc);
+    if (slabs.size() + 1 > ctx->ev_in.size() || slabs.size() > ctx->ev_out.size())
+        return fail(ctx, GKS_ETOOBIG, "pipelined step: more slabs than events");
     struct Cur {
         long long done, end;
     };
@@ -427,7 +455,9 @@ int evolve_slabs(gks_ctx *ctx, double *const W[5])
         c.done = ready;
         return r;
     };
-    std::vector<std::pair<long long, long long>> out_planes; // physical planes downloaded after slab k
+    // padded host planes downloaded after slab k
+    std::vector<std::vector<std::pair<long long, long long>>> out_planes;
+    bool top_ghosts = false;
     for (size_t k = 0; k < slabs.size(); ++k) {
         const long long a = slabs[k].first, b = slabs[k].second;
         const bool all = k + 1 == slabs.size();
@@ -480,24 +510,28 @@ int evolve_slabs(gks_ctx *ctx, double *const W[5])
         FieldDev dn = d;
         for (int q = 0; q < 5; ++q) dn.W[q] = d.Wout[q];
         const long long u1 = upd.done;
-        if (u1 > u0) CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, (u0 + 3) * P, (u1 + 3) * P));
-        if (all) { // the y ghost planes: the periodic images of planes nc-3 .. nc-1 and 0 .. 2
-            CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, 0, 3 * P));
+        std::vector<std::pair<long long, long long>> rng;
+        if (u1 > u0) {
+            CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, (u0 + 3) * P, (u1 + 3) * P));
+            rng.push_back({u0 + 3, u1 + 3});
+        }
+        if (!top_ghosts && u1 >= 3) { // the top y ghost planes: the periodic images of planes 0 .. 2
             CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, (nt - 3) * P, Nt));
+            rng.push_back({nt - 3, nt});
+            top_ghosts = true;
+        }
+        if (all) { // the bottom ones: the images of planes nc-3 .. nc-1
+            CK(gks::launch_scatter(dn, ctx->d_stage_out, ctx->nsm, ctx->stream, 0, 3 * P));
+            rng.push_back({0, 3});
         }
         CK(cudaEventRecord(ctx->ev_out[k], ctx->stream));
-        out_planes.push_back({u0 + 3, u1 + 3});
+        out_planes.push_back(rng);
     }
     // downloads, each after its slab's update (enqueued after all uploads and
     // stages, so that a blocking copy into pageable memory holds up nothing)
     for (size_t k = 0; k < out_planes.size(); ++k) {
         CK(cudaStreamWaitEvent(ctx->d2h, ctx->ev_out[k], 0));
-        std::vector<std::pair<long long, long long>> rng{out_planes[k]};
-        if (k + 1 == out_planes.size()) {
-            rng.push_back({0, 3});
-            rng.push_back({nt - 3, nt});
-        }
-        for (auto pr : rng) {
+        for (auto pr : out_planes[k]) {
             if (pr.second <= pr.first) continue;
             const size_t off = (size_t)pr.first * P, bytes = (size_t)(pr.second - pr.first) * P * sizeof(double);
             if (contiguous) {

@@ -23,7 +23,7 @@ def plain(gks, case, W, prec, dt, nsteps=1, flags=0):
         return s.download()
 
 
-@pytest.mark.parametrize("nc", [16, 19, 40, 64, 100])
+@pytest.mark.parametrize("nc", [16, 19, 40, 64, 100, 130])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_pipelined_evolve_equals_upload_step_download(gks, nc, prec):
     case = gks_ic.make_dhit(nc, k0=4.0, Mt=0.4, Re_lambda=80.0, seed=nc)
