@@ -172,3 +172,20 @@ def test_slab_field_over_a_one_rank_nccl_group(gks):
         want = s.stats()
     for k in gks.STATS_FIELDS:
         assert st[k] == pytest.approx(want[k], rel=1e-13, abs=1e-15)
+
+
+@pytest.mark.parametrize("mode", [["--local-slabs", "2"], ["--slabs"]])
+def test_bench_slab_modes_print_a_line(mode):
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ)
+    env.pop("MASTER_PORT", None)
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), *mode, "--nc", "32", "--steps", "2",
+                        "--warmup", "3", "--no-tune"], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    assert line["value"] > 0 and line["scaling"] == "strong"
+    assert line["config"]["slabs"] == (2 if mode[0] == "--local-slabs" else 1)
