@@ -40,6 +40,14 @@ struct FieldHost {
     // reconstruction buffers (10 + 10) -- made on first use
     double *pipe = nullptr;
     double *spare[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // Lagrangian particles (gks_particles_*): one allocation of the nprt
+    // particle records (GKS_PREC_FIELDS doubles each, field-major) followed by
+    // the statistics scratch; and, made by the first gks_particles_props, the
+    // spline coefficients of the five primitives over the padded block
+    // (5 (nc+8)^3 doubles) followed by the nc + 8 pivots of their line solves
+    double *prt = nullptr;
+    long long nprt = 0;
+    double *coef = nullptr;
     bool uploaded = false;
     bool have_dt = false;
 };
@@ -765,6 +773,8 @@ void gks_destroy(gks_ctx *ctx)
         if (h.spl) cudaFree(h.spl);
         if (h.pipe) cudaFree(h.pipe);
         if (h.halo) cudaFree(h.halo);
+        if (h.prt) cudaFree(h.prt);
+        if (h.coef) cudaFree(h.coef);
     }
     if (ctx->d_fields) cudaFree(ctx->d_fields);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
@@ -1005,6 +1015,126 @@ int gks_stats(gks_ctx *ctx, int f, gks_stats_out *out)
     if (rc) return rc;
     if (!out) return fail(ctx, GKS_EINVAL, "null output");
     return gks_stats_reduce(part, 1, &ctx->fh[f].phys, out);
+}
+
+// ---------------------------------------------------------------------------
+// Lagrangian particles of one periodic field (kernels in gks_particles.cu).
+// ---------------------------------------------------------------------------
+int gks_particles_locate(gks_ctx *ctx, int f, int n, const double *x0, const double *y0, const double *z0)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    FieldHost &h = ctx->fh[f];
+    if (h.slab) return fail(ctx, GKS_EINVAL, "particles: a y-slab is not a whole periodic field");
+    if (n < 1 || !x0 || !y0 || !z0) return fail(ctx, GKS_EINVAL, "particles: need n >= 1 and three position arrays");
+    for (int a = 0; a < n; ++a)
+        if (!std::isfinite(x0[a]) || !std::isfinite(y0[a]) || !std::isfinite(z0[a]))
+            return fail(ctx, GKS_EINVAL, "particles: non-finite initial position");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream)); // earlier work may still read the old records
+    const size_t rec = (size_t)GKS_PREC_FIELDS * n;
+    if (h.nprt != n) {
+        if (h.prt) cudaFree(h.prt);
+        h.prt = nullptr;
+        h.nprt = 0;
+        if (cudaMalloc(&h.prt, (rec + gks::particle_partial_elems(ctx->nsm) + 8) * sizeof(double)) != cudaSuccess) {
+            h.prt = nullptr;
+            return fail(ctx, GKS_ENOMEM, "particle records allocation failed");
+        }
+        h.nprt = n;
+    }
+    // a new Particle holds zeros (Particle::Particle, ParticleTrack.cpp:6-10),
+    // its position pos[0..2] = (y0, x0, z0) (initializeParticle, :12-18)
+    CK(cudaMemsetAsync(h.prt, 0, rec * sizeof(double), ctx->stream));
+    const double *src[3] = {y0, x0, z0};
+    for (int q = 0; q < 3; ++q)
+        CK(cudaMemcpyAsync(h.prt + (size_t)q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GKS_OK;
+}
+
+int gks_particles_props(gks_ctx *ctx, int f)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    FieldHost &h = ctx->fh[f];
+    if (!h.nprt) return fail(ctx, GKS_ESTATE, "particles: props before gks_particles_locate");
+    if (!h.uploaded) return fail(ctx, GKS_ESTATE, "particles: props before upload");
+    CK(cudaSetDevice(ctx->device));
+    const long long nt = h.phys.nc + 6, M = nt + 2, M3 = M * M * M;
+    if (!h.coef) {
+        if (cudaMalloc(&h.coef, (5 * M3 + M) * sizeof(double)) != cudaSuccess) {
+            h.coef = nullptr;
+            return fail(ctx, GKS_ENOMEM, "particle spline coefficients allocation failed");
+        }
+        // pivots of the (1, 4, 1) eliminations along lines of nt nodes
+        std::vector<double> w(M, 0.0);
+        w[2] = 0.25;
+        for (long long m = 3; m < nt; ++m) w[m] = 1.0 / (4.0 - w[m - 1]);
+        CK(cudaMemcpy(h.coef + 5 * M3, w.data(), M * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // the spline grid of the padded block (get_bsplinep, Interpolation.cpp:10-27,
+    // sta = 0): nt nodes from -3 dx + dx/2, spacing (end - start) / (nt - 1)
+    const double dx = h.dev.dx;
+    const double start = (0 - 3) * dx + 0.5 * dx, end = start + (nt - 1) * dx;
+    const double hinv = 1.0 / ((end - start) / (double)(nt - 1));
+    CK(gks::launch_particle_splines(h.dev, h.coef, h.coef + 5 * M3, ctx->nsm, ctx->stream));
+    CK(gks::launch_particle_props(h.dev, h.coef, start, hinv, h.prt, h.nprt, ctx->nsm, ctx->stream));
+    return GKS_OK;
+}
+
+int gks_particles_track(gks_ctx *ctx, int f, double dt)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    FieldHost &h = ctx->fh[f];
+    if (!h.nprt) return fail(ctx, GKS_ESTATE, "particles: track before gks_particles_locate");
+    if (!std::isfinite(dt)) return fail(ctx, GKS_EINVAL, "particles: dt must be finite");
+    CK(cudaSetDevice(ctx->device));
+    const double twopi = 2 * std::atan(1.0) * 4.0; // 2*pi as param.h:14 defines pi
+    CK(gks::launch_particle_track(h.prt, h.nprt, dt, twopi, ctx->nsm, ctx->stream));
+    return GKS_OK;
+}
+
+int gks_particles_stats(gks_ctx *ctx, int f, gks_particle_stats_out *out)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    FieldHost &h = ctx->fh[f];
+    if (!out) return fail(ctx, GKS_EINVAL, "null output");
+    if (!h.nprt) return fail(ctx, GKS_ESTATE, "particles: stats before gks_particles_locate");
+    CK(cudaSetDevice(ctx->device));
+    double *partial = h.prt + (size_t)GKS_PREC_FIELDS * h.nprt;
+    double *sums = partial + gks::particle_partial_elems(ctx->nsm);
+    CK(gks::launch_particle_stats(h.prt, h.nprt, partial, sums, ctx->nsm, ctx->stream));
+    double m[6];
+    CK(cudaMemcpyAsync(m, sums, sizeof(m), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // normalisation of GetParticleStats (update.cpp:1168-1175)
+    out->tke = m[0];
+    out->sijsij = m[1];
+    out->dudx2 = m[2];
+    out->dudx3 = m[3];
+    out->dwdz2 = m[4];
+    out->dwdz3 = m[5];
+    out->skew_u = m[3] / std::pow(m[2], 1.5);
+    out->skew_w = m[5] / std::pow(m[4], 1.5);
+    out->count = h.nprt;
+    return GKS_OK;
+}
+
+int gks_particles_get(gks_ctx *ctx, int f, double *rec)
+{
+    int rc = check_field(ctx, f);
+    if (rc) return rc;
+    FieldHost &h = ctx->fh[f];
+    if (!rec) return fail(ctx, GKS_EINVAL, "null output");
+    if (!h.nprt) return fail(ctx, GKS_ESTATE, "particles: get before gks_particles_locate");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(rec, h.prt, (size_t)GKS_PREC_FIELDS * h.nprt * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GKS_OK;
 }
 
 int gks_halo_buffers(gks_ctx *ctx, double **bufs, size_t *elems)

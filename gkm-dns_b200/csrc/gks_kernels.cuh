@@ -151,6 +151,20 @@ cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int 
 // (K = the values at the first interior cell).
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st);
 
+// Lagrangian particles of one periodic field (gks_particles.cu).  coef: five
+// arrays of (nc + 8)^3 doubles (the natural cubic B-spline coefficients of
+// den, u, v, w, p over the padded block), w: the nc + 8 pivots of the line
+// solves; rec: GKS_PREC_FIELDS x n doubles, field-major.  The statistics write
+// the six means TKE, SijSij, DUDX2, DUDX3, DWDZ2, DWDZ3 into sums[0..5]
+// (partial: particle_partial_elems(nsm) doubles).
+cudaError_t launch_particle_splines(const FieldDev &f, double *coef, const double *w, int nsm, cudaStream_t st);
+cudaError_t launch_particle_props(const FieldDev &f, const double *coef, double start, double hinv, double *rec,
+                                  long long n, int nsm, cudaStream_t st);
+cudaError_t launch_particle_track(double *rec, long long n, double dt, double twopi, int nsm, cudaStream_t st);
+cudaError_t launch_particle_stats(const double *rec, long long n, double *partial, double *sums, int nsm,
+                                  cudaStream_t st);
+int particle_partial_elems(int nsm);
+
 // Scan a field's interior planes for non-finite values or non-positive density / pressure; sets bit 1 of *err.
 cudaError_t launch_check(const FieldDev &f, int *err, int nsm, cudaStream_t st);
 

@@ -63,8 +63,21 @@ class StatsOut(ctypes.Structure):
                          self.sijsij, self.mach_t, self.rho_mean])
 
 
+class ParticleStatsOut(ctypes.Structure):
+    _fields_ = [
+        ("tke", ctypes.c_double), ("sijsij", ctypes.c_double), ("dudx2", ctypes.c_double),
+        ("dudx3", ctypes.c_double), ("dwdz2", ctypes.c_double), ("dwdz3", ctypes.c_double),
+        ("skew_u", ctypes.c_double), ("skew_w", ctypes.c_double), ("count", ctypes.c_longlong),
+    ]
+
+    def as_array(self) -> np.ndarray:
+        return np.array([self.tke, self.sijsij, self.dudx2, self.dudx3, self.dwdz2, self.dwdz3, self.skew_u,
+                         self.skew_w, float(self.count)])
+
+
 DP = ctypes.POINTER(ctypes.c_double)
 DP5 = DP * 5
+PREC_FIELDS = 23  # GKS_PREC_FIELDS: doubles of one particle record
 
 # every symbol the header declares, with (restype, argtypes)
 SIGNATURES = {
@@ -103,6 +116,11 @@ SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_size_t)]),
     "gks_halo_pack": (ctypes.c_int, [ctypes.c_void_p]),
     "gks_halo_unpack": (ctypes.c_int, [ctypes.c_void_p]),
+    "gks_particles_locate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, DP, DP, DP]),
+    "gks_particles_props": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "gks_particles_track": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]),
+    "gks_particles_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ParticleStatsOut)]),
+    "gks_particles_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, DP]),
 }
 
 STATS_PART = 28  # doubles of one gks_stats_part record
@@ -287,6 +305,37 @@ class Solver:
         out = np.empty(STATS_PART)
         self._ck(self._lib.gks_stats_part(self._h, f, out.ctypes.data_as(DP)))
         return out
+
+    # Lagrangian particles -----------------------------------------------------
+    def particles_locate(self, x0: np.ndarray, y0: np.ndarray, z0: np.ndarray, f: int = 0):
+        """Place len(x0) particles at (x0, y0, z0) (locateParticles; the three
+        arrays of InitialConditions/unirand), velocity and properties zero."""
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x0, y0, z0)]
+        if not (xs[0].size == xs[1].size == xs[2].size):
+            raise ValueError("x0, y0, z0 must have the same length")
+        self._ck(self._lib.gks_particles_locate(self._h, f, xs[0].size, *[a.ctypes.data_as(DP) for a in xs]))
+        self._np = getattr(self, "_np", {})
+        self._np[f] = xs[0].size
+
+    def particles_props(self, f: int = 0):
+        """Splines of the current state and every particle's values and gradients (asynchronous)."""
+        self._ck(self._lib.gks_particles_props(self._h, f))
+
+    def particles_track(self, dt: float, f: int = 0):
+        """Move every particle by dt with the velocity of the last props call (asynchronous)."""
+        self._ck(self._lib.gks_particles_track(self._h, f, dt))
+
+    def particles_stats(self, f: int = 0) -> np.ndarray:
+        """GetParticleStats: TKE, SijSij, DUDX2, DUDX3, DWDZ2, DWDZ3, SKEWu, SKEWw, count."""
+        out = ParticleStatsOut()
+        self._ck(self._lib.gks_particles_stats(self._h, f, ctypes.byref(out)))
+        return out.as_array()
+
+    def particles_get(self, f: int = 0) -> np.ndarray:
+        """The particle records, (PREC_FIELDS, n) doubles (field-major)."""
+        rec = np.empty((PREC_FIELDS, self._np[f]))
+        self._ck(self._lib.gks_particles_get(self._h, f, rec.ctypes.data_as(DP)))
+        return rec
 
     # halo exchange of a slab ------------------------------------------------
     def halo_buffers(self) -> tuple:

@@ -249,6 +249,54 @@ int gks_set_launch(gks_ctx *ctx, int kind, int dir, int grid, int variant);
  * the current device in TFLOP/s, 2 flops per FMA (a short microbenchmark). */
 int gks_peak_flops(int precision, double *tflops);
 
+/* Lagrangian particles of field f (a whole periodic field, not a y-slab),
+ * replacing the reference's particle tracker on one rank:
+ *   locateParticles (reads InitialConditions/unirand)  weno/src/update.cpp:1269-1292
+ *   generateSplines + Particle::getParticleProp        weno/src/update.cpp:1199-1213,
+ *                                                      ParticleTrack.cpp:90-97
+ *   evolveParticles / Particle::track (one rank)        weno/src/update.cpp:1082-1131,
+ *                                                      ParticleTrack.cpp:38-65
+ *   GetParticleStats                                    weno/src/update.cpp:1134-1181
+ * (the reference defines these but its Evolve loop never calls them).
+ * A particle record holds GKS_PREC_FIELDS doubles; gks_particles_get returns
+ * them field-major (field q of particle a at rec[q*n + a]):
+ *   0-2   position pos[0..2] = (y, x, z), in [0, 2 pi]
+ *   3     DEN           4-6  U[0..2] = (u, v, w)      7  P
+ *   8-10  gradD (d/dy, d/dx, d/dz)   11-13 gradU   14-16 gradV
+ *   17-19 gradW         20-22 gradP
+ * Values and gradients come from the natural cubic B-spline interpolant of
+ * the primitives over the padded block (einspline's UBspline_3d_d with
+ * NATURAL ends, as get_bsplinep builds it, Interpolation.cpp:3-31).
+ *
+ * gks_particles_locate: n particles at (x0[a], y0[a], z0[a]) -- the three
+ * arrays of InitialConditions/unirand in the order the reference reads them
+ * -- with zero velocity and properties; replaces the field's particles.
+ * gks_particles_props: the splines of the field's current state and every
+ * particle's values and gradients (asynchronous on the context's stream; the
+ * first call allocates 5 (nc+8)^3 doubles of spline coefficients).
+ * gks_particles_track: every particle moves by dt with the velocity of the
+ * last props call (forward Euler, each coordinate wrapped into [0, 2 pi], as
+ * Particle::updatePosition); asynchronous.
+ * gks_particles_stats: GetParticleStats' means over the particles
+ * (synchronises).  gks_particles_get: the records into host memory
+ * (GKS_PREC_FIELDS x n doubles; synchronises). */
+#define GKS_PREC_FIELDS 23
+
+typedef struct {
+    double tke;            /* <|U|^2> over the particles (part_TKE; no factor 1/2, update.cpp:1144) */
+    double sijsij;         /* <S_ij S_ij> (part_SijSij) */
+    double dudx2, dudx3;   /* <(du/dx)^2>, <(du/dx)^3> */
+    double dwdz2, dwdz3;   /* <(dw/dz)^2>, <(dw/dz)^3> */
+    double skew_u, skew_w; /* part_SKEWu, part_SKEWw */
+    long long count;       /* particles (totalCount) */
+} gks_particle_stats_out;
+
+int gks_particles_locate(gks_ctx *ctx, int f, int n, const double *x0, const double *y0, const double *z0);
+int gks_particles_props(gks_ctx *ctx, int f);
+int gks_particles_track(gks_ctx *ctx, int f, double dt);
+int gks_particles_stats(gks_ctx *ctx, int f, gks_particle_stats_out *out);
+int gks_particles_get(gks_ctx *ctx, int f, double *rec);
+
 /* The time step without allocating anything -- for callers that may not
  * allocate device memory: host codes that own and pool every byte of device
  * memory themselves, and loops that cannot afford cudaMalloc's implicit

@@ -711,3 +711,240 @@ void orc_stats_ranks(const double *W, const orc_params *p, int nranks, double *o
 }
 
 void orc_stats(const double *W, const orc_params *p, double *out) { orc_stats_ranks(W, p, 1, out); }
+
+/* ---------------------------------------------------------------------------
+ * Lagrangian particles (weno/src/ParticleTrack.cpp, update.cpp:1082-1303).
+ *
+ * The reference interpolates the primitives at a particle with einspline's
+ * 3-D cubic B-spline under natural boundary conditions (get_bsplinep,
+ * Interpolation.cpp:3-31; eval_UBspline_3d_d_vg in getParticleProp,
+ * ParticleTrack.cpp:90-97).  einspline is an external library that is absent
+ * here (no version pinned, weno/makefileGPU:4,7,13); its construction is
+ * restated from the mathematics.  On a uniform grid of N nodes
+ * x_n = start + n h the interpolant is
+ *   s(x) = sum_{m=0}^{N+1} c_m beta(u - m + 1),   u = (x - start) / h,
+ * with beta the centred cubic B-spline (beta(0) = 2/3, beta(+-1) = 1/6) and
+ *   (c_n + 4 c_{n+1} + c_{n+2}) / 6 = f_n,          n = 0 .. N-1 (interpolation)
+ *   c_0 - 2 c_1 + c_2 = 0 = c_{N-1} - 2 c_N + c_{N+1}   (s'' = 0 at both ends).
+ * The end conditions with the first and last interpolation rows give
+ * c_1 = f_0 and c_N = f_{N-1}; c_2 .. c_{N-1} solve the tridiagonal system of
+ * rows (1, 4, 1) with right-hand sides 6 f_{m-1} (the first and last less the
+ * known c_1, c_N), by forward elimination with the pivots w_2 = 1/4,
+ * w_m = 1/(4 - w_{m-1}), and back substitution; then c_0 = 2 c_1 - c_2 and
+ * c_{N+1} = 2 c_N - c_{N-1}.  In 3-D the coefficients are the tensor product:
+ * the same solve along z, then x, then y.
+ * ------------------------------------------------------------------------- */
+void orc_bspline_pivots(long N, double *w)
+{
+    for (long m = 0; m < N + 2; ++m) w[m] = 0.0;
+    w[2] = 0.25;
+    for (long m = 3; m < N; ++m) w[m] = 1.0 / (4.0 - w[m - 1]);
+}
+
+/* One line: c[m * stride], m = 1 .. N, hold f_{m-1} on entry (N >= 4). */
+static void bspline_line(long N, double *c, long stride, const double *w)
+{
+    const double f0 = c[stride], fl = c[N * stride];
+    double d = (6.0 * c[2 * stride] - f0) * w[2];
+    c[2 * stride] = d;
+    for (long m = 3; m < N - 1; ++m) {
+        d = (6.0 * c[m * stride] - d) * w[m];
+        c[m * stride] = d;
+    }
+    d = ((6.0 * c[(N - 1) * stride] - fl) - d) * w[N - 1];
+    c[(N - 1) * stride] = d;
+    for (long m = N - 2; m >= 2; --m) c[m * stride] = c[m * stride] - w[m] * c[(m + 1) * stride];
+    c[0] = 2.0 * f0 - c[2 * stride];
+    c[(N + 1) * stride] = 2.0 * fl - c[(N - 1) * stride];
+}
+
+void orc_bspline3(long N0, long N1, long N2, const double *data, double *coef)
+{
+    const long M0 = N0 + 2, M1 = N1 + 2, M2 = N2 + 2;
+    const long Nmax = N0 > N1 ? (N0 > N2 ? N0 : N2) : (N1 > N2 ? N1 : N2);
+    double *w = (double *)malloc(sizeof(double) * (size_t)(Nmax + 2));
+    for (long a = 0; a < M0 * M1 * M2; ++a) coef[a] = 0.0;
+    for (long j = 0; j < N0; ++j)
+        for (long i = 0; i < N1; ++i)
+            for (long k = 0; k < N2; ++k) coef[((j + 1) * M1 + (i + 1)) * M2 + (k + 1)] = data[(j * N1 + i) * N2 + k];
+    orc_bspline_pivots(N2, w);
+    for (long j = 1; j <= N0; ++j)
+        for (long i = 1; i <= N1; ++i) bspline_line(N2, coef + (j * M1 + i) * M2, 1, w);
+    orc_bspline_pivots(N1, w);
+    for (long j = 1; j <= N0; ++j)
+        for (long k = 0; k < M2; ++k) bspline_line(N1, coef + j * M1 * M2 + k, M2, w);
+    orc_bspline_pivots(N0, w);
+    for (long i = 0; i < M1; ++i)
+        for (long k = 0; k < M2; ++k) bspline_line(N0, coef + i * M2 + k, M1 * M2, w);
+    free(w);
+}
+
+/* Cell index and basis weights (values b, derivatives db with respect to u)
+ * of position x on a grid of num nodes; the index is clamped to the last
+ * interval. */
+static long bspline_weights(double x, double start, double hinv, long num, double b[4], double db[4])
+{
+    const double u = (x - start) * hinv;
+    long i = (long)floor(u);
+    if (i < 0) i = 0;
+    if (i > num - 2) i = num - 2;
+    const double t = u - (double)i;
+    const double s = 1.0 - t, t2 = t * t, t3 = t2 * t;
+    b[0] = (s * s * s) / 6.0;
+    b[1] = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
+    b[2] = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
+    b[3] = t3 / 6.0;
+    db[0] = -0.5 * (s * s);
+    db[1] = 1.5 * t2 - 2.0 * t;
+    db[2] = (-1.5 * t2 + t) + 0.5;
+    db[3] = 0.5 * t2;
+    return i;
+}
+
+/* Value and gradient (axes 0, 1, 2) of the tensor-product spline with
+ * coefficients C (dims M1, M2 of the two faster axes) at the cell i0[3] with
+ * the weights of each axis. */
+static void bspline_eval(const double *C, long M1, long M2, const long i0[3], const double by[4],
+                         const double dby[4], const double bx[4], const double dbx[4], const double bz[4],
+                         const double dbz[4], const double hinv[3], double *val, double g[3])
+{
+    double v = 0.0, gy = 0.0, gx = 0.0, gz = 0.0;
+    for (int a = 0; a < 4; ++a) {
+        double va = 0.0, gxa = 0.0, gza = 0.0;
+        for (int b = 0; b < 4; ++b) {
+            const double *r = C + ((i0[0] + a) * M1 + (i0[1] + b)) * M2 + i0[2];
+            const double s = ((bz[0] * r[0] + bz[1] * r[1]) + bz[2] * r[2]) + bz[3] * r[3];
+            const double sd = ((dbz[0] * r[0] + dbz[1] * r[1]) + dbz[2] * r[2]) + dbz[3] * r[3];
+            va += bx[b] * s;
+            gxa += dbx[b] * s;
+            gza += bx[b] * sd;
+        }
+        v += by[a] * va;
+        gy += dby[a] * va;
+        gx += by[a] * gxa;
+        gz += by[a] * gza;
+    }
+    *val = v;
+    g[0] = gy * hinv[0];
+    g[1] = gx * hinv[1];
+    g[2] = gz * hinv[2];
+}
+
+void orc_spline_eval(long N0, long N1, long N2, const double *coef, const double start[3], const double hinv[3],
+                     long n, const double *pos, double *val, double *grad)
+{
+    const long num[3] = {N0, N1, N2};
+    for (long p = 0; p < n; ++p) {
+        double b[3][4], db[3][4];
+        long i0[3];
+        for (int a = 0; a < 3; ++a) i0[a] = bspline_weights(pos[a * n + p], start[a], hinv[a], num[a], b[a], db[a]);
+        double g[3];
+        bspline_eval(coef, N1 + 2, N2 + 2, i0, b[0], db[0], b[1], db[1], b[2], db[2], hinv, &val[p], g);
+        for (int a = 0; a < 3; ++a) grad[a * n + p] = g[a];
+    }
+}
+
+/* The spline grid of one rank's padded block along an axis (get_bsplinep,
+ * Interpolation.cpp:10-27): nt nodes from (sta - 3) dx + dx/2; einspline
+ * derives the spacing from the end points, (end - start) / (num - 1). */
+static void particle_grid(const orc_params *p, double *start, double *hinv)
+{
+    const long nt = p->nc + 6;
+    const double st = (0 - 3) * p->dx + 0.5 * p->dx; /* sta = 0 on one rank */
+    const double en = st + (nt - 1) * p->dx;
+    *start = st;
+    *hinv = 1.0 / ((en - st) / (double)(nt - 1));
+}
+
+/* generateSplines (update.cpp:1199-1213) over the padded block W (ghosts
+ * filled), then getParticleProp (ParticleTrack.cpp:90-97) at every particle.
+ * rec: ORC_PREC_FIELDS x n doubles, field-major; fields 0-2 (position
+ * y, x, z = pos[0..2]) are read, 3-22 written: DEN, U[0..2], P and the
+ * gradients (d/dy, d/dx, d/dz) of DEN, U[0], U[1], U[2], P. */
+void orc_particle_props(const double *W, const orc_params *p, long n, double *rec)
+{
+    const long nt = p->nc + 6, Nt = nt * nt * nt, M = nt + 2;
+    double *prim5 = (double *)malloc(sizeof(double) * (size_t)(5 * Nt));
+    double *coef = (double *)malloc(sizeof(double) * (size_t)(M * M * M));
+    for (long c = 0; c < Nt; ++c) {
+        const double den = W[c];
+        const double u = W[Nt + c] / den, v = W[2 * Nt + c] / den, w = W[3 * Nt + c] / den;
+        const double Vsqr = u * u + v * v + w * w;
+        prim5[c] = den;
+        prim5[Nt + c] = u;
+        prim5[2 * Nt + c] = v;
+        prim5[3 * Nt + c] = w;
+        prim5[4 * Nt + c] = (den * (p->gam - 1)) * (W[4 * Nt + c] / den - 0.5 * Vsqr);
+    }
+    double start, hinv;
+    particle_grid(p, &start, &hinv);
+    const double st3[3] = {start, start, start}, hi3[3] = {hinv, hinv, hinv};
+    double *val = (double *)malloc(sizeof(double) * (size_t)n);
+    double *grad = (double *)malloc(sizeof(double) * (size_t)(3 * n));
+    for (int q = 0; q < 5; ++q) {
+        orc_bspline3(nt, nt, nt, prim5 + q * Nt, coef);
+        orc_spline_eval(nt, nt, nt, coef, st3, hi3, n, rec, val, grad);
+        for (long a = 0; a < n; ++a) {
+            rec[(3 + q) * n + a] = val[a];
+            for (int d = 0; d < 3; ++d) rec[(8 + 3 * q + d) * n + a] = grad[d * n + a];
+        }
+    }
+    free(grad);
+    free(val);
+    free(coef);
+    free(prim5);
+}
+
+/* Particle::updatePosition (ParticleTrack.cpp:43-65): forward Euler with the
+ * velocity of the last getParticleProp (pos[0] = y moves with U[1] = v,
+ * pos[1] = x with U[0] = u), each coordinate wrapped once into [0, 2 pi]. */
+void orc_particle_track(long n, double *rec, double dt)
+{
+    const double twopi = 2 * atan(1.0) * 4.0; /* 2*pi with param.h:14's pi */
+    for (long a = 0; a < n; ++a) {
+        double *py = rec + a, *px = rec + n + a, *pz = rec + 2 * n + a;
+        *py += rec[5 * n + a] * dt;
+        *px += rec[4 * n + a] * dt;
+        *pz += rec[6 * n + a] * dt;
+        double *pp[3] = {py, px, pz};
+        for (int q = 0; q < 3; ++q) {
+            if (*pp[q] > twopi) *pp[q] = *pp[q] - twopi;
+            if (*pp[q] < 0) *pp[q] = twopi + *pp[q];
+        }
+    }
+}
+
+/* GetParticleStats (update.cpp:1134-1181) on one rank: out[9] = part_TKE,
+ * part_SijSij, DUDX2, DUDX3, DWDZ2, DWDZ3, part_SKEWu, part_SKEWw, count. */
+void orc_particle_stats(long n, const double *rec, double *out)
+{
+    double tke = 0.0, sij = 0.0, d2 = 0.0, d3 = 0.0, w2 = 0.0, w3 = 0.0;
+    for (long a = 0; a < n; ++a) {
+        const double U0 = rec[4 * n + a], U1 = rec[5 * n + a], U2 = rec[6 * n + a];
+        tke += (U0 * U0 + U1 * U1 + U2 * U2);
+        const double dudy = rec[11 * n + a], dudx = rec[12 * n + a], dudz = rec[13 * n + a];
+        const double dvdy = rec[14 * n + a], dvdx = rec[15 * n + a], dvdz = rec[16 * n + a];
+        const double dwdy = rec[17 * n + a], dwdx = rec[18 * n + a], dwdz = rec[19 * n + a];
+        sij += (dudx * dudx + 0.5 * pow(dudy + dvdx, 2) + 0.5 * pow(dudz + dwdx, 2) + 0.5 * pow(dwdy + dvdz, 2) +
+                dvdy * dvdy + dwdz * dwdz);
+        d2 += dudx * dudx;
+        d3 += dudx * dudx * dudx;
+        w2 += dwdz * dwdz;
+        w3 += dwdz * dwdz * dwdz;
+    }
+    tke /= n;
+    sij /= n;
+    d2 /= n;
+    d3 /= n;
+    w2 /= n;
+    w3 /= n;
+    out[0] = tke;
+    out[1] = sij;
+    out[2] = d2;
+    out[3] = d3;
+    out[4] = w2;
+    out[5] = w3;
+    out[6] = d3 / pow(d2, 1.5);
+    out[7] = w3 / pow(w2, 1.5);
+    out[8] = (double)n;
+}

@@ -80,6 +80,37 @@ void orc_stats(const double *W, const orc_params *p, double *out);
  * reference's PrintStats does with MPI (update.cpp:638-784). */
 void orc_stats_ranks(const double *W, const orc_params *p, int nranks, double *out);
 
+
+/* Lagrangian particles (ParticleTrack.cpp, update.cpp:1082-1303), restated
+ * from the mathematics of einspline's natural cubic B-spline (see
+ * gks_oracle.c).  A particle record holds ORC_PREC_FIELDS doubles, stored
+ * field-major (field f of particle a at f*n + a): 0-2 position (y, x, z), 3 DEN,
+ * 4-6 U (u, v, w), 7 P, then (d/dy, d/dx, d/dz) of DEN (8-10), u (11-13),
+ * v (14-16), w (17-19), P (20-22). */
+#define ORC_PREC_FIELDS 23
+
+/* Pivots w[0 .. N+1] of the (1, 4, 1) elimination (w[2] .. w[N-1] used). */
+void orc_bspline_pivots(long N, double *w);
+
+/* Natural cubic B-spline coefficients of data[N0][N1][N2] into
+ * coef[N0+2][N1+2][N2+2] (N0, N1, N2 >= 4). */
+void orc_bspline3(long N0, long N1, long N2, const double *data, double *coef);
+
+/* Value and gradient of that spline at n points pos[3][n] (axes 0, 1, 2) on
+ * grids start[a] + m / hinv[a]: val[n], grad[3][n]. */
+void orc_spline_eval(long N0, long N1, long N2, const double *coef, const double start[3], const double hinv[3],
+                     long n, const double *pos, double *val, double *grad);
+
+/* generateSplines + getParticleProp of every particle (positions in rec). */
+void orc_particle_props(const double *W, const orc_params *p, long n, double *rec);
+
+/* Particle::updatePosition of every particle. */
+void orc_particle_track(long n, double *rec, double dt);
+
+/* GetParticleStats: out[9] = TKE, SijSij, DUDX2, DUDX3, DWDZ2, DWDZ3, SKEWu,
+ * SKEWw, particle count. */
+void orc_particle_stats(long n, const double *rec, double *out);
+
 #ifdef __cplusplus
 }
 #endif

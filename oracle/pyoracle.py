@@ -69,6 +69,12 @@ def lib():
         L.orc_maxval.restype = ctypes.c_double
         L.orc_stats.argtypes = [dp, ctypes.POINTER(OrcParams), dp]
         L.orc_stats_ranks.argtypes = [dp, ctypes.POINTER(OrcParams), ctypes.c_int, dp]
+        L.orc_bspline3.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, dp, dp]
+        L.orc_spline_eval.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, dp, dp, dp, ctypes.c_long,
+                                      dp, dp, dp]
+        L.orc_particle_props.argtypes = [dp, ctypes.POINTER(OrcParams), ctypes.c_long, dp]
+        L.orc_particle_track.argtypes = [ctypes.c_long, dp, ctypes.c_double]
+        L.orc_particle_stats.argtypes = [ctypes.c_long, dp, dp]
         _lib = L
     return _lib
 
@@ -138,6 +144,52 @@ def stats_ranks(W: np.ndarray, prm: OrcParams, nranks: int) -> np.ndarray:
 def halo(W: np.ndarray, nc: int) -> np.ndarray:
     lib().orc_halo(_p(W), nc)
     return W
+
+
+# --- Lagrangian particles (orc_bspline3 ... orc_particle_stats) -------------
+
+PREC_FIELDS = 23  # ORC_PREC_FIELDS
+
+
+def bspline3(data: np.ndarray) -> np.ndarray:
+    """Natural cubic B-spline coefficients (N0+2, N1+2, N2+2) of data (N0, N1, N2)."""
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    c = np.empty(tuple(n + 2 for n in d.shape))
+    lib().orc_bspline3(d.shape[0], d.shape[1], d.shape[2], _p(d), _p(c))
+    return c
+
+
+def spline_eval(coef: np.ndarray, start, hinv, pos: np.ndarray):
+    """Value (n,) and gradient (3, n) of the spline at pos (3, n)."""
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    x = np.ascontiguousarray(pos, dtype=np.float64)
+    n = x.shape[1]
+    val = np.empty(n)
+    grad = np.empty((3, n))
+    st = np.asarray(start, dtype=np.float64)
+    hi = np.asarray(hinv, dtype=np.float64)
+    N = [s - 2 for s in c.shape]
+    lib().orc_spline_eval(N[0], N[1], N[2], _p(c), _p(st), _p(hi), n, _p(x), _p(val), _p(grad))
+    return val, grad
+
+
+def particle_props(W: np.ndarray, prm: OrcParams, rec: np.ndarray) -> np.ndarray:
+    """Fill fields 3..22 of the particle records rec (23, n) from the padded block W (ghosts filled)."""
+    assert rec.shape[0] == PREC_FIELDS and rec.flags["C_CONTIGUOUS"]
+    lib().orc_particle_props(_p(np.ascontiguousarray(W)), ctypes.byref(prm), rec.shape[1], _p(rec))
+    return rec
+
+
+def particle_track(rec: np.ndarray, dt: float) -> np.ndarray:
+    assert rec.shape[0] == PREC_FIELDS and rec.flags["C_CONTIGUOUS"]
+    lib().orc_particle_track(rec.shape[1], _p(rec), dt)
+    return rec
+
+
+def particle_stats(rec: np.ndarray) -> np.ndarray:
+    out = np.empty(9)
+    lib().orc_particle_stats(rec.shape[1], _p(np.ascontiguousarray(rec)), _p(out))
+    return out
 
 
 # --- the reference build ---------------------------------------------------
