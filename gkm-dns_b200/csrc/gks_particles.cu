@@ -11,9 +11,9 @@
 //   * k_node_prims: the five primitives (den, u, v, w, p) at the (nc+6)^3
 //     nodes of the padded block -- the ghost nodes as the periodic image --
 //     written into the interior of five coefficient arrays of (nc+8)^3;
-//   * k_bspline_lines<AXIS>: the natural cubic B-spline coefficients, one
-//     tridiagonal (1, 4, 1) solve per grid line, along z, then x, then y (the
-//     tensor product).  With c_1 = f_0 and c_N = f_{N-1} fixed by the natural
+//   * k_bspline_zlines, k_bspline_lines<AXIS>: the natural cubic B-spline
+//     coefficients, one tridiagonal (1, 4, 1) solve per grid line, along z,
+//     then x, then y (the tensor product).  With c_1 = f_0 and c_N = f_{N-1} fixed by the natural
 //     end conditions, c_2 .. c_{N-1} come from forward elimination with the
 //     host-computed pivots w_2 = 1/4, w_m = 1/(4 - w_{m-1}) and back
 //     substitution, then c_0 = 2 c_1 - c_2 and c_{N+1} = 2 c_N - c_{N-1};
@@ -98,32 +98,112 @@ __device__ __forceinline__ void bspline_line(long long N, double *c, long long s
     c[(N + 1) * s] = 2.0 * fl - cl;
 }
 
-// One pass of line solves over all five arrays along AXIS (0 y, 1 x, 2 z);
-// lines of the later passes include the end coefficients of the earlier ones.
+// One pass of line solves over all five arrays along AXIS (0 y, 1 x): a
+// thread per line, consecutive threads on consecutive lines (k fastest), so
+// that every access of a warp is one contiguous run; the lines include the
+// end coefficients of the passes before (x pass N M lines per array, y pass
+// M^2).
 template <int AXIS>
 __global__ void __launch_bounds__(kLineBlock) k_bspline_lines(double *coef, long long N, const double *w)
 {
+    static_assert(AXIS == 0 || AXIS == 1, "the z pass is k_bspline_zlines");
     const long long M = N + 2, M3 = M * M * M;
-    // lines per array: z pass N^2 (rows 1..N of y and x), x pass N M, y pass M^2
-    const long long L = AXIS == 2 ? N * N : (AXIS == 1 ? N * M : M * M);
+    const long long L = AXIS == 1 ? N * M : M * M;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 5 * L; t += stride) {
         const long long q = t / L, l = t - q * L;
-        double *base;
-        long long s;
-        if (AXIS == 2) {
-            const long long j = 1 + l / N, i = 1 + l % N;
-            base = coef + q * M3 + (j * M + i) * M;
-            s = 1;
-        } else if (AXIS == 1) {
+        if (AXIS == 1) {
             const long long j = 1 + l / M, k = l % M;
-            base = coef + q * M3 + j * M * M + k;
-            s = M;
+            bspline_line(N, coef + q * M3 + j * M * M + k, M, w);
         } else {
-            base = coef + q * M3 + l;
-            s = M * M;
+            bspline_line(N, coef + q * M3 + l, M * M, w);
         }
-        bspline_line(N, base, s, w);
+    }
+}
+
+// The z pass, whose lines are contiguous: a block takes kZLines lines and moves
+// them through shared memory in tiles of kZChunk positions (each line's
+// positions read and written as contiguous runs), each thread running its own
+// line's recurrences -- the arithmetic of bspline_line, chunk by chunk:
+// forward elimination over increasing positions, back substitution and the
+// two end coefficients over decreasing ones.
+constexpr int kZLines = 128;
+constexpr int kZChunk = 32;
+
+__global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long long N, const double *__restrict__ w)
+{
+    __shared__ double tile[kZLines][kZChunk + 1];
+    __shared__ double *lbase[kZLines];
+    const long long M = N + 2, M3 = M * M * M, L = N * N, total = 5 * L;
+    const int t = threadIdx.x;
+    const long long nchunk = (M + kZChunk - 1) / kZChunk;
+    for (long long l0 = (long long)blockIdx.x * kZLines; l0 < total; l0 += (long long)gridDim.x * kZLines) {
+        const long long l = l0 + t;
+        const bool mine = l < total;
+        double *line = nullptr;
+        if (mine) {
+            const long long q = l / L, r = l - q * L;
+            line = coef + q * M3 + ((1 + r / N) * M + (1 + r % N)) * M;
+        }
+        lbase[t] = line;
+        double f0 = 0.0, fl = 0.0, d = 0.0;
+        if (mine) {
+            f0 = line[1];
+            fl = line[N];
+        }
+        __syncthreads();
+        // tile [line][position] <-> global, each line's run of positions contiguous
+        auto move = [&](long long p0, bool load) {
+            for (int idx = t; idx < kZLines * kZChunk; idx += kZLines) {
+                const int ln = idx / kZChunk, e = idx - ln * kZChunk;
+                double *b = lbase[ln];
+                if (b && p0 + e < M) {
+                    if (load) tile[ln][e] = b[p0 + e];
+                    else b[p0 + e] = tile[ln][e];
+                }
+            }
+        };
+        for (long long c = 0; c < nchunk; ++c) {
+            const long long p0 = c * kZChunk;
+            move(p0, true);
+            __syncthreads();
+            if (mine) {
+                for (int e = 0; e < kZChunk; ++e) {
+                    const long long m = p0 + e;
+                    if (m < 2 || m > N - 1) continue;
+                    if (m == 2) d = (6.0 * tile[t][e] - f0) * __ldg(w + 2);
+                    else if (m < N - 1) d = (6.0 * tile[t][e] - d) * __ldg(w + m);
+                    else d = ((6.0 * tile[t][e] - fl) - d) * __ldg(w + N - 1);
+                    tile[t][e] = d;
+                }
+            }
+            __syncthreads();
+            move(p0, false);
+            __syncthreads();
+        }
+        const double cl = d; // c_{N-1}
+        double cn = d;
+        for (long long c = nchunk - 1; c >= 0; --c) {
+            const long long p0 = c * kZChunk;
+            move(p0, true);
+            __syncthreads();
+            if (mine) {
+                for (int e = kZChunk - 1; e >= 0; --e) {
+                    const long long m = p0 + e;
+                    if (m == N + 1) {
+                        tile[t][e] = 2.0 * fl - cl;
+                    } else if (m >= 2 && m <= N - 2) {
+                        cn = tile[t][e] - __ldg(w + m) * cn;
+                        tile[t][e] = cn;
+                    } else if (m == 0) {
+                        tile[t][e] = 2.0 * f0 - cn; // cn = c_2 here
+                    }
+                }
+            }
+            __syncthreads();
+            move(p0, false);
+            __syncthreads();
+        }
     }
 }
 
@@ -277,7 +357,7 @@ cudaError_t launch_particle_splines(const FieldDev &f, double *coef, const doubl
 {
     const long long nt = f.nc + 6, M = nt + 2;
     k_node_prims<<<grid_for(nt * nt * nt, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(f, coef);
-    k_bspline_lines<2><<<grid_for(5 * nt * nt, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
+    k_bspline_zlines<<<grid_for(5 * nt * nt, kZLines, nsm, 6), kZLines, 0, st>>>(coef, nt, w);
     k_bspline_lines<1><<<grid_for(5 * nt * M, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
     k_bspline_lines<0><<<grid_for(5 * M * M, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
     return cudaGetLastError();
