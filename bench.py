@@ -537,6 +537,34 @@ def run_ours(args):
     for _ in range(3):
         s.stats()
     stats_ms = (time.perf_counter() - t0s) / 3 * 1e3
+    # the Lagrangian particle tracker on the same field (generateSplines +
+    # getParticleProp for every particle, then one track), CUDA events on the
+    # solver's stream
+    prt = None
+    if not args.no_particles:
+        import numpy as np
+
+        npart = 1 << 20
+        rng = np.random.default_rng(7)
+        s.particles_locate(*(rng.random(npart) * 2 * np.pi for _ in range(3)))
+        pst = torch.cuda.ExternalStream(s.stream())
+        s.particles_props()  # allocates the spline coefficients
+        s.particles_track(1e-3)
+        s.sync()
+        pe = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        pe[0].record(pst)
+        for _ in range(3):
+            s.particles_props()
+        pe[1].record(pst)
+        for _ in range(3):
+            s.particles_track(1e-3)
+        pe[2].record(pst)
+        pe[2].synchronize()
+        prt = {"particles": npart, "props_ms": pe[0].elapsed_time(pe[1]) / 3,
+               "track_ms": pe[1].elapsed_time(pe[2]) / 3,
+               "what": "gks_particles_props (natural cubic B-splines of den, u, v, w, p over the padded "
+                       f"{nc + 6}^3 block + value and gradient at every particle) and gks_particles_track, "
+                       "uniformly random positions"}
     s.close()
 
     ens = None
@@ -654,6 +682,7 @@ def run_ours(args):
                     "peak_gbs": hbm_peak, "peak_source": hbm_src,
                     "note": "compulsory 80 B/cell-update; the path is FP64-pipe bound"},
             "stage_ms": stages["fp64"], "recon_ms": recon_ms, "stats_ms": stats_ms,
+            "particles": prt,
             "ensemble": ens,
             "launch": {"fp64": results["fp64"]["launch"], "mixed": results["mixed"]["launch"],
                        "tuned": not args.no_tune},
@@ -796,6 +825,7 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 96-field ensemble line")
     ap.add_argument("--no-refgpu", action="store_true", help="skip timing the reference's own GPU path")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the mixed-vs-FP64 run to t/t0 = 2")
+    ap.add_argument("--no-particles", action="store_true", help="skip timing the Lagrangian particle tracker")
     ap.add_argument("--accuracy", action="store_true", help="mixed vs FP64 statistics to t/t0 = --t-end, then exit")
     ap.add_argument("--t-end", type=float, default=2.0, help="accuracy run length in eddy turnover times")
     ap.add_argument("--control", action="store_true",
