@@ -252,6 +252,29 @@ def cpu_baseline(nc: int, steps: int, warmup: int, planes: int = 8, procs: int =
                       f"{planes}x{nc}x{nc} y-slab of the {nc}^3 field per process, {procs} process(es)"}
 
 
+def particle_cpu_baseline(W, case, npart: int) -> dict:
+    """The oracle's particle routine (orc_particle_props: natural cubic
+    B-splines of the five primitives over the padded block, then value and
+    gradient at every particle) on one host core, on the same field and number
+    of particles as the GPU figure.  A port, not the reference: the
+    reference's tracker needs einspline, which is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+
+    prm = pyoracle.params(case.nc, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    rng = np.random.default_rng(7)
+    rec = np.zeros((pyoracle.PREC_FIELDS, npart))
+    for q in range(3):
+        rec[q] = rng.random(npart) * 2 * np.pi
+    t0 = time.perf_counter()
+    pyoracle.particle_props(W, prm, rec)
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"props_ms": ms, "cores": 1, "kind": "port",
+            "sample": f"one orc_particle_props call (gcc -O2) on the same {case.nc}^3 field with {npart} "
+                      "particles"}
+
+
 def reference_gpu(nc: int, steps: int, warmup: int) -> dict | None:
     """The reference's own GPU path on the same field: GPUupdate.cu and GPUAlloc.cu
     built for sm_100a (oracle/_ref/ref_gpu_harness).  Each of its steps is evolve()
@@ -648,6 +671,8 @@ def run_ours(args):
         cb = cpu_baseline(nc, 1, 1, planes=8, procs=1)
     if rank == 0 and ws == 1 and not args.no_refgpu:
         rg = reference_gpu(nc, 3, 1)
+    if prt and rank == 0 and ws == 1 and not args.no_cpu:
+        prt["cpu_baseline"] = particle_cpu_baseline(W, case, prt["particles"])
 
     if rank == 0:
         line = {
