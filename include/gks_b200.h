@@ -266,7 +266,8 @@ int gks_peak_flops(int precision, double *tflops);
  *   17-19 gradW         20-22 gradP
  * Values and gradients come from the natural cubic B-spline interpolant of
  * the primitives over the padded block (einspline's UBspline_3d_d with
- * NATURAL ends, as get_bsplinep builds it, Interpolation.cpp:3-31).
+ * NATURAL ends, as get_bsplinep builds it, Interpolation.cpp:3-31), in FP64
+ * whatever the context's precision.
  *
  * gks_particles_locate: n particles at (x0[a], y0[a], z0[a]) -- the three
  * arrays of InitialConditions/unirand in the order the reference reads them

@@ -171,3 +171,31 @@ def test_particles_at_256_follow_a_uniform_stream(gks):
         st = s.particles_stats()
         np.testing.assert_allclose(st[0], sum(u * u for u in U), rtol=1e-12)
         assert st[8] == n
+
+
+def test_particles_on_an_ensemble_field_and_after_the_host_step(gks, oracle):
+    """Particles belong to one field of a context: on the second field of an
+    ensemble they see that field only; after gks_evolve (the pipelined host
+    step, which swaps the field's state buffers) they see the new state."""
+    cases = [setup(nc, nc + 50, 700) for nc in (18, 26)]
+    with gks.Solver([gks.phys_from_case(c[0]) for c in cases]) as s:
+        for f, (case, W, *_) in enumerate(cases):
+            s.upload(W, f)
+        case, W, x0, y0, z0 = cases[1]
+        s.particles_locate(x0, y0, z0, f=1)
+        s.particles_props(f=1)
+        _, want = oracle_records(oracle, case, W, x0, y0, z0)
+        assert np.array_equal(s.particles_get(f=1), want)
+        with pytest.raises(gks.GksError) as ei:
+            s.particles_props(f=0)  # field 0 has no particles
+        assert ei.value.code == -4
+    case, W, x0, y0, z0 = setup(32, 8, 900)
+    with gks.Solver(gks.phys_from_case(case)) as s:
+        s.upload(W)
+        dt = s.timestep(0.5)
+        host = W.copy()
+        s.evolve(host)  # one field, one step: the slab-pipelined form
+        s.particles_locate(x0, y0, z0)
+        s.particles_props()
+        _, want = oracle_records(oracle, case, host, x0, y0, z0)  # host: the new state, ghosts filled
+        assert np.array_equal(s.particles_get(), want)
