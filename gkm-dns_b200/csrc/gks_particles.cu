@@ -74,23 +74,50 @@ __global__ void __launch_bounds__(kLineBlock) k_node_prims(FieldDev f, double *c
 
 // Natural cubic B-spline coefficients of one grid line in place:
 // c[m * s], m = 1 .. N, hold the data f_{m-1} on entry (N >= 4).
+// Both recurrences move through the line in groups of kLineGroup positions,
+// every load of a group issued before its first use, so that a thread keeps
+// kLineGroup loads in flight instead of one (the recurrences themselves are
+// sequential).
+constexpr int kLineGroup = 8;
+
 __device__ __forceinline__ void bspline_line(long long N, double *c, long long s, const double *__restrict__ w)
 {
     const double f0 = c[s], fl = c[N * s];
     double d = (6.0 * c[2 * s] - f0) * __ldg(w + 2);
     c[2 * s] = d;
-    double nxt = c[3 * s];
-    for (long long m = 3; m < N - 1; ++m) {
-        const double cur = nxt;
-        nxt = c[(m + 1) * s]; // the next datum, loaded before this one's store
-        d = (6.0 * cur - d) * __ldg(w + m);
+    // forward elimination over m = 3 .. N-2, then the last row m = N-1
+    long long m = 3;
+    for (; m + kLineGroup <= N - 1; m += kLineGroup) {
+        double v[kLineGroup];
+#pragma unroll
+        for (int g = 0; g < kLineGroup; ++g) v[g] = c[(m + g) * s];
+#pragma unroll
+        for (int g = 0; g < kLineGroup; ++g) {
+            d = (6.0 * v[g] - d) * __ldg(w + m + g);
+            c[(m + g) * s] = d;
+        }
+    }
+    for (; m < N - 1; ++m) {
+        d = (6.0 * c[m * s] - d) * __ldg(w + m);
         c[m * s] = d;
     }
-    d = ((6.0 * nxt - fl) - d) * __ldg(w + N - 1);
+    d = ((6.0 * c[(N - 1) * s] - fl) - d) * __ldg(w + N - 1);
     c[(N - 1) * s] = d;
     const double cl = d; // c_{N-1}
     double cn = d;
-    for (long long m = N - 2; m >= 2; --m) {
+    // back substitution over m = N-2 .. 2
+    m = N - 2;
+    for (; m - kLineGroup + 1 >= 2; m -= kLineGroup) {
+        double v[kLineGroup];
+#pragma unroll
+        for (int g = 0; g < kLineGroup; ++g) v[g] = c[(m - g) * s];
+#pragma unroll
+        for (int g = 0; g < kLineGroup; ++g) {
+            cn = v[g] - __ldg(w + m - g) * cn;
+            c[(m - g) * s] = cn;
+        }
+    }
+    for (; m >= 2; --m) {
         cn = c[m * s] - __ldg(w + m) * cn;
         c[m * s] = cn;
     }
@@ -152,14 +179,29 @@ __global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long l
             fl = line[N];
         }
         __syncthreads();
-        // tile [line][position] <-> global, each line's run of positions contiguous
+        // tile [line][position] <-> global, each line's run of positions
+        // contiguous; a load issues all of a thread's kZChunk reads before the
+        // first shared-memory write, so that they are in flight together
         auto move = [&](long long p0, bool load) {
-            for (int idx = t; idx < kZLines * kZChunk; idx += kZLines) {
-                const int ln = idx / kZChunk, e = idx - ln * kZChunk;
-                double *b = lbase[ln];
-                if (b && p0 + e < M) {
-                    if (load) tile[ln][e] = b[p0 + e];
-                    else b[p0 + e] = tile[ln][e];
+            if (load) {
+                double v[kZChunk];
+#pragma unroll
+                for (int r = 0; r < kZChunk; ++r) {
+                    const int idx = t + r * kZLines, ln = idx / kZChunk, e = idx - ln * kZChunk;
+                    const double *b = lbase[ln];
+                    v[r] = (b && p0 + e < M) ? b[p0 + e] : 0.0;
+                }
+#pragma unroll
+                for (int r = 0; r < kZChunk; ++r) {
+                    const int idx = t + r * kZLines, ln = idx / kZChunk, e = idx - ln * kZChunk;
+                    tile[ln][e] = v[r];
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < kZChunk; ++r) {
+                    const int idx = t + r * kZLines, ln = idx / kZChunk, e = idx - ln * kZChunk;
+                    double *b = lbase[ln];
+                    if (b && p0 + e < M) b[p0 + e] = tile[ln][e];
                 }
             }
         };
@@ -168,13 +210,16 @@ __global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long l
             move(p0, true);
             __syncthreads();
             if (mine) {
+#pragma unroll
                 for (int e = 0; e < kZChunk; ++e) {
                     const long long m = p0 + e;
-                    if (m < 2 || m > N - 1) continue;
-                    if (m == 2) d = (6.0 * tile[t][e] - f0) * __ldg(w + 2);
-                    else if (m < N - 1) d = (6.0 * tile[t][e] - d) * __ldg(w + m);
-                    else d = ((6.0 * tile[t][e] - fl) - d) * __ldg(w + N - 1);
-                    tile[t][e] = d;
+                    const double x = tile[t][e], wm = __ldg(w + (m < M ? m : M - 1));
+                    if (m >= 2 && m <= N - 1) {
+                        if (m == 2) d = (6.0 * x - f0) * wm;
+                        else if (m < N - 1) d = (6.0 * x - d) * wm;
+                        else d = ((6.0 * x - fl) - d) * wm;
+                        tile[t][e] = d;
+                    }
                 }
             }
             __syncthreads();
@@ -188,12 +233,14 @@ __global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long l
             move(p0, true);
             __syncthreads();
             if (mine) {
+#pragma unroll
                 for (int e = kZChunk - 1; e >= 0; --e) {
                     const long long m = p0 + e;
+                    const double x = tile[t][e], wm = __ldg(w + (m < M ? m : M - 1));
                     if (m == N + 1) {
                         tile[t][e] = 2.0 * fl - cl;
                     } else if (m >= 2 && m <= N - 2) {
-                        cn = tile[t][e] - __ldg(w + m) * cn;
+                        cn = x - wm * cn;
                         tile[t][e] = cn;
                     } else if (m == 0) {
                         tile[t][e] = 2.0 * f0 - cn; // cn = c_2 here
