@@ -632,8 +632,8 @@ __device__ __forceinline__ void flux_item(const FieldDev &f, long long it, S (*p
 // A batch of one field reads the field's descriptor from the launch
 // parameters (b.one: constant-bank operands, nothing loaded per interface);
 // an ensemble looks each interface's field up in the device array.
-template <int DIR, int PREC, int MINB>
-__global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(Batch b)
+template <int DIR, int PREC, int REGS>
+__global__ void __launch_bounds__(kFluxBlock) __maxnreg__(REGS) k_flux(Batch b)
 {
     using S = typename std::conditional<PREC == 0, double, float>::type;
     __shared__ S park_dw[15][kFluxBlock];
@@ -1118,13 +1118,16 @@ cudaError_t occ(KernelT k, int block, int *n)
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k, block, 0);
 }
 
-// Register-cap variants (min resident blocks per SM: reconstruction blocks of
-// 128 threads at 3 / 4 / 5 -> 168 / 128 / 96 registers, each in the windowed
-// and the one-interface form, flux blocks of 64 threads at
-// 5 / 6 / 7 -> 204 / 168 / 146 registers); the tuner picks one per
-// kernel, precision and sweep.  Every variant gives bit-identical results.
+// Register-cap variants: reconstruction blocks of 128 threads at 3 / 4 / 5
+// resident blocks per SM (launch bounds; 168 / 128 / 96 registers), each in
+// the windowed and the one-interface form; flux blocks of 64 threads at
+// explicit caps of 200 / 168 / 128 registers (5 / 6 / 8 resident blocks).  A
+// launch bound of 5 blocks of 64 threads would not give the 200: the compiler
+// rounds the resident warps up to a multiple of four and caps at 168, as for
+// 6 blocks.  The tuner picks one variant per kernel, precision and sweep.
+// Every variant gives bit-identical results.
 constexpr int kReconMinb[3] = {3, 4, 5};
-constexpr int kFluxMinb[kFluxVariants] = {5, 6, 7};
+constexpr int kFluxRegs[kFluxVariants] = {200, 168, 128};
 
 // The item range of a launch (all items of its kind when b.hi < 0) and the
 // blocks it needs: at most cfg.grid, no more than the range fills.
@@ -1184,9 +1187,9 @@ cudaError_t flux_go(Batch b, LaunchCfg cfg, cudaStream_t st)
     if (b.hi <= b.lo) return cudaSuccess;
     const int g = range_grid(cfg.grid, b.hi - b.lo, cfg.block);
     switch (cfg.variant) {
-    case 1: k_flux<DIR, PREC, kFluxMinb[1]><<<g, cfg.block, 0, st>>>(b); break;
-    case 2: k_flux<DIR, PREC, kFluxMinb[2]><<<g, cfg.block, 0, st>>>(b); break;
-    default: k_flux<DIR, PREC, kFluxMinb[0]><<<g, cfg.block, 0, st>>>(b); break;
+    case 1: k_flux<DIR, PREC, kFluxRegs[1]><<<g, cfg.block, 0, st>>>(b); break;
+    case 2: k_flux<DIR, PREC, kFluxRegs[2]><<<g, cfg.block, 0, st>>>(b); break;
+    default: k_flux<DIR, PREC, kFluxRegs[0]><<<g, cfg.block, 0, st>>>(b); break;
     }
     return cudaGetLastError();
 }
@@ -1210,9 +1213,9 @@ cudaError_t occ_kind(int kind, int variant, int block, int *n)
         if (variant % 3 == 2) return occ(k_recon<DIR, PREC, kReconMinb[2]>, block, n);
         return occ(k_recon<DIR, PREC, kReconMinb[0]>, block, n);
     }
-    if (variant == 1) return occ(k_flux<DIR, PREC, kFluxMinb[1]>, block, n);
-    if (variant == 2) return occ(k_flux<DIR, PREC, kFluxMinb[2]>, block, n);
-    return occ(k_flux<DIR, PREC, kFluxMinb[0]>, block, n);
+    if (variant == 1) return occ(k_flux<DIR, PREC, kFluxRegs[1]>, block, n);
+    if (variant == 2) return occ(k_flux<DIR, PREC, kFluxRegs[2]>, block, n);
+    return occ(k_flux<DIR, PREC, kFluxRegs[0]>, block, n);
 }
 
 template <int PREC>
