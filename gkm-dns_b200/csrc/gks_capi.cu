@@ -44,7 +44,8 @@ struct FieldHost {
     // particle records (GKS_PREC_FIELDS doubles each, field-major) followed by
     // the statistics scratch; and, made by the first gks_particles_props, the
     // spline coefficients of the five primitives over the padded block
-    // (5 (nc+8)^3 doubles) followed by the nc + 8 pivots of their line solves
+    // (5 (nc+8)^3 doubles, interleaved per node) followed by the nc + 8 pivots
+    // of their line solves
     double *prt = nullptr;
     long long nprt = 0;
     double *coef = nullptr;

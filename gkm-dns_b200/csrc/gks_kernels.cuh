@@ -151,9 +151,9 @@ cudaError_t launch_maxwave(const FieldDev &f, unsigned long long *out_bits, int 
 // (K = the values at the first interior cell).
 cudaError_t launch_stats(const FieldDev &f, double *scratch, double *partial, double *sums, int nsm, cudaStream_t st);
 
-// Lagrangian particles of one periodic field (gks_particles.cu).  coef: five
-// arrays of (nc + 8)^3 doubles (the natural cubic B-spline coefficients of
-// den, u, v, w, p over the padded block), w: the nc + 8 pivots of the line
+// Lagrangian particles of one periodic field (gks_particles.cu).  coef:
+// 5 (nc + 8)^3 doubles, the natural cubic B-spline coefficients of den, u, v,
+// w, p over the padded block, the five fields interleaved per node, w: the nc + 8 pivots of the line
 // solves; rec: GKS_PREC_FIELDS x n doubles, field-major.  The statistics write
 // the six means TKE, SijSij, DUDX2, DUDX3, DWDZ2, DWDZ3 into sums[0..5]
 // (partial: particle_partial_elems(nsm) doubles).

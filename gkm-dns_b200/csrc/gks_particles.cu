@@ -10,7 +10,9 @@
 // from the resident state:
 //   * k_node_prims: the five primitives (den, u, v, w, p) at the (nc+6)^3
 //     nodes of the padded block -- the ghost nodes as the periodic image --
-//     written into the interior of five coefficient arrays of (nc+8)^3;
+//     written into the interior of one coefficient array of (nc+8)^3 nodes
+//     with the five fields interleaved per node (node-major, so that the 4 x 4
+//     x 4 block a particle reads is 16 runs of 20 contiguous doubles);
 //   * k_bspline_zlines, k_bspline_lines<AXIS>: the natural cubic B-spline
 //     coefficients, one tridiagonal (1, 4, 1) solve per grid line, along z,
 //     then x, then y (the tensor product).  With c_1 = f_0 and c_N = f_{N-1} fixed by the natural
@@ -42,16 +44,17 @@ constexpr int kPrtBlock = 128;
 constexpr int kLineBlock = 128;
 constexpr int kSumBlock = 256;
 constexpr int kNSum = 6; // TKE, SijSij, DUDX2, DUDX3, DWDZ2, DWDZ3
+constexpr int kNF = 5;   // fields interleaved per node: den, u, v, w, p
 
 __device__ __forceinline__ int wrap_nc(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 
 // generateSplines' primitives at every node of the padded block
-// (update.cpp:1201-1208): den, u, v, w, p, into the coefficient arrays at
-// offset (1, 1, 1).
+// (update.cpp:1201-1208): den, u, v, w, p, into the coefficient array at
+// node offset (1, 1, 1).
 __global__ void __launch_bounds__(kLineBlock) k_node_prims(FieldDev f, double *coef)
 {
     const int nc = f.nc;
-    const long long nt = nc + 6, M = nt + 2, M3 = M * M * M, N3 = nt * nt * nt;
+    const long long nt = nc + 6, M = nt + 2, N3 = nt * nt * nt;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const double gm1 = f.gam - 1;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < N3; c += stride) {
@@ -63,12 +66,12 @@ __global__ void __launch_bounds__(kLineBlock) k_node_prims(FieldDev f, double *c
         const double u = f.W[1][cell] / den, v = f.W[2][cell] / den, w = f.W[3][cell] / den;
         const double Vsqr = u * u + v * v + w * w;
         const double p = (den * gm1) * (f.W[4][cell] / den - 0.5 * Vsqr);
-        const long long o = ((long long)(j + 1) * M + (i + 1)) * M + (k + 1);
-        coef[o] = den;
-        coef[M3 + o] = u;
-        coef[2 * M3 + o] = v;
-        coef[3 * M3 + o] = w;
-        coef[4 * M3 + o] = p;
+        double *o = coef + kNF * (((long long)(j + 1) * M + (i + 1)) * M + (k + 1));
+        o[0] = den;
+        o[1] = u;
+        o[2] = v;
+        o[3] = w;
+        o[4] = p;
     }
 }
 
@@ -125,83 +128,91 @@ __device__ __forceinline__ void bspline_line(long long N, double *c, long long s
     c[(N + 1) * s] = 2.0 * fl - cl;
 }
 
-// One pass of line solves over all five arrays along AXIS (0 y, 1 x): a
-// thread per line, consecutive threads on consecutive lines (k fastest), so
-// that every access of a warp is one contiguous run; the lines include the
-// end coefficients of the passes before (x pass N M lines per array, y pass
+// One pass of line solves over all five fields along AXIS (0 y, 1 x): a
+// thread per line and field, consecutive threads on consecutive (k, field),
+// so that every access of a warp is one contiguous run; the lines include the
+// end coefficients of the passes before (x pass N M lines per field, y pass
 // M^2).
 template <int AXIS>
 __global__ void __launch_bounds__(kLineBlock) k_bspline_lines(double *coef, long long N, const double *w)
 {
     static_assert(AXIS == 0 || AXIS == 1, "the z pass is k_bspline_zlines");
-    const long long M = N + 2, M3 = M * M * M;
-    const long long L = AXIS == 1 ? N * M : M * M;
+    const long long M = N + 2;
+    const long long L = kNF * (AXIS == 1 ? N * M : M * M);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 5 * L; t += stride) {
-        const long long q = t / L, l = t - q * L;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += stride) {
         if (AXIS == 1) {
-            const long long j = 1 + l / M, k = l % M;
-            bspline_line(N, coef + q * M3 + j * M * M + k, M, w);
+            // t = ((j - 1) M + k) kNF + q: element m of the line at ((j M + m) M + k) kNF + q
+            const long long l = t / kNF, q = t - l * kNF, j = 1 + l / M, k = l % M;
+            bspline_line(N, coef + (j * M * M + k) * kNF + q, M * kNF, w);
         } else {
-            bspline_line(N, coef + q * M3 + l, M * M, w);
+            // t = (i M + k) kNF + q: element m at ((m M + i) M + k) kNF + q
+            bspline_line(N, coef + t, M * M * kNF, w);
         }
     }
 }
 
-// The z pass, whose lines are contiguous: a block takes kZLines lines and moves
-// them through shared memory in tiles of kZChunk positions (each line's
-// positions read and written as contiguous runs), each thread running its own
-// line's recurrences -- the arithmetic of bspline_line, chunk by chunk:
-// forward elimination over increasing positions, back substitution and the
-// two end coefficients over decreasing ones.
-constexpr int kZLines = 128;
+// The z pass, whose lines are contiguous: a block takes kZRows grid rows
+// (j, i) with their kNF interleaved fields and moves them through shared
+// memory in tiles of kZChunk positions -- a row's chunk is one contiguous run
+// of kNF kZChunk doubles -- each thread running the recurrences of one row
+// and field: the arithmetic of bspline_line, chunk by chunk, forward
+// elimination over increasing positions, back substitution and the two end
+// coefficients over decreasing ones.  The tile's row pitch (kZPitch = 5 mod
+// 16 doubles) keeps a half-warp's accesses, thread t at row t / 5 and field
+// t % 5, on distinct banks.
+constexpr int kZRows = 32;
+constexpr int kZThreads = kNF * kZRows;
 constexpr int kZChunk = 32;
+constexpr int kZRun = kNF * kZChunk;     // doubles of one row's chunk
+constexpr int kZPitch = kZRun + 5;       // 165 = 5 mod 16
+constexpr int kZBatch = 16;              // reads of a thread in flight at once
 
-__global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long long N, const double *__restrict__ w)
+__global__ void __launch_bounds__(kZThreads) k_bspline_zlines(double *coef, long long N, const double *__restrict__ w)
 {
-    __shared__ double tile[kZLines][kZChunk + 1];
-    __shared__ double *lbase[kZLines];
-    const long long M = N + 2, M3 = M * M * M, L = N * N, total = 5 * L;
-    const int t = threadIdx.x;
+    __shared__ double tile[kZRows][kZPitch];
+    __shared__ double *rbase[kZRows];
+    const long long M = N + 2, R = N * N;
+    const int t = threadIdx.x, r = t / kNF, q = t - r * kNF;
     const long long nchunk = (M + kZChunk - 1) / kZChunk;
-    for (long long l0 = (long long)blockIdx.x * kZLines; l0 < total; l0 += (long long)gridDim.x * kZLines) {
-        const long long l = l0 + t;
-        const bool mine = l < total;
-        double *line = nullptr;
-        if (mine) {
-            const long long q = l / L, r = l - q * L;
-            line = coef + q * M3 + ((1 + r / N) * M + (1 + r % N)) * M;
-        }
-        lbase[t] = line;
-        double f0 = 0.0, fl = 0.0, d = 0.0;
-        if (mine) {
-            f0 = line[1];
-            fl = line[N];
+    for (long long r0 = (long long)blockIdx.x * kZRows; r0 < R; r0 += (long long)gridDim.x * kZRows) {
+        if (t < kZRows) {
+            const long long rr = r0 + t; // row (1 + rr / N, 1 + rr % N)
+            rbase[t] = rr < R ? coef + ((1 + rr / N) * M + (1 + rr % N)) * M * kNF : nullptr;
         }
         __syncthreads();
-        // tile [line][position] <-> global, each line's run of positions
-        // contiguous; a load issues all of a thread's kZChunk reads before the
-        // first shared-memory write, so that they are in flight together
+        const bool mine = rbase[r] != nullptr;
+        const double *line = mine ? rbase[r] + q : nullptr; // element m at line[m * kNF]
+        double f0 = 0.0, fl = 0.0, d = 0.0;
+        if (mine) {
+            f0 = line[kNF];
+            fl = line[N * kNF];
+        }
+        // tile <-> global: each row's chunk [p0, p0 + kZChunk) x fields is one run
         auto move = [&](long long p0, bool load) {
+            const long long lim = (M - p0) * kNF; // doubles of the row left from p0
             if (load) {
-                double v[kZChunk];
 #pragma unroll
-                for (int r = 0; r < kZChunk; ++r) {
-                    const int idx = t + r * kZLines, ln = idx / kZChunk, e = idx - ln * kZChunk;
-                    const double *b = lbase[ln];
-                    v[r] = (b && p0 + e < M) ? b[p0 + e] : 0.0;
-                }
+                for (int h = 0; h < kZRows * kZRun / kZThreads; h += kZBatch) {
+                    double v[kZBatch];
 #pragma unroll
-                for (int r = 0; r < kZChunk; ++r) {
-                    const int idx = t + r * kZLines, ln = idx / kZChunk, e = idx - ln * kZChunk;
-                    tile[ln][e] = v[r];
+                    for (int b = 0; b < kZBatch; ++b) {
+                        const int idx = t + (h + b) * kZThreads, rw = idx / kZRun, e = idx - rw * kZRun;
+                        const double *bp = rbase[rw];
+                        v[b] = (bp && e < lim) ? bp[p0 * kNF + e] : 0.0;
+                    }
+#pragma unroll
+                    for (int b = 0; b < kZBatch; ++b) {
+                        const int idx = t + (h + b) * kZThreads, rw = idx / kZRun, e = idx - rw * kZRun;
+                        tile[rw][e] = v[b];
+                    }
                 }
             } else {
 #pragma unroll
-                for (int r = 0; r < kZChunk; ++r) {
-                    const int idx = t + r * kZLines, ln = idx / kZChunk, e = idx - ln * kZChunk;
-                    double *b = lbase[ln];
-                    if (b && p0 + e < M) b[p0 + e] = tile[ln][e];
+                for (int h = 0; h < kZRows * kZRun / kZThreads; ++h) {
+                    const int idx = t + h * kZThreads, rw = idx / kZRun, e = idx - rw * kZRun;
+                    double *bp = rbase[rw];
+                    if (bp && e < lim) bp[p0 * kNF + e] = tile[rw][e];
                 }
             }
         };
@@ -213,12 +224,12 @@ __global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long l
 #pragma unroll
                 for (int e = 0; e < kZChunk; ++e) {
                     const long long m = p0 + e;
-                    const double x = tile[t][e], wm = __ldg(w + (m < M ? m : M - 1));
+                    const double x = tile[r][e * kNF + q], wm = __ldg(w + (m < M ? m : M - 1));
                     if (m >= 2 && m <= N - 1) {
                         if (m == 2) d = (6.0 * x - f0) * wm;
                         else if (m < N - 1) d = (6.0 * x - d) * wm;
                         else d = ((6.0 * x - fl) - d) * wm;
-                        tile[t][e] = d;
+                        tile[r][e * kNF + q] = d;
                     }
                 }
             }
@@ -236,14 +247,14 @@ __global__ void __launch_bounds__(kZLines) k_bspline_zlines(double *coef, long l
 #pragma unroll
                 for (int e = kZChunk - 1; e >= 0; --e) {
                     const long long m = p0 + e;
-                    const double x = tile[t][e], wm = __ldg(w + (m < M ? m : M - 1));
+                    const double x = tile[r][e * kNF + q], wm = __ldg(w + (m < M ? m : M - 1));
                     if (m == N + 1) {
-                        tile[t][e] = 2.0 * fl - cl;
+                        tile[r][e * kNF + q] = 2.0 * fl - cl;
                     } else if (m >= 2 && m <= N - 2) {
                         cn = x - wm * cn;
-                        tile[t][e] = cn;
+                        tile[r][e * kNF + q] = cn;
                     } else if (m == 0) {
-                        tile[t][e] = 2.0 * f0 - cn; // cn = c_2 here
+                        tile[r][e * kNF + q] = 2.0 * f0 - cn; // cn = c_2 here
                     }
                 }
             }
@@ -277,43 +288,65 @@ __device__ __forceinline__ int bspline_weights(double x, double start, double hi
 }
 
 // getParticleProp (ParticleTrack.cpp:90-97) of every particle: value and
-// gradient of the five splines at its position.
+// gradient of the five splines at its position.  A row of the 4 x 4 x 4
+// coefficient block -- four nodes along z with their five fields -- is one
+// contiguous run of 20 doubles, read once for all fields; each field's sums
+// keep the order of a field-by-field evaluation (rows along y, then x, nodes
+// along z innermost).  Measured alternatives: the five fields in separate
+// arrays read 8.4 GB of DRAM per 2^20 particles at 256^3 (1.43 ms) against
+// 4.1 GB here (1.65 ms, latency-bound at 8 warps per SM: the 35 sums and the
+// row take 254 registers; capped at 168 they spill and take 1.74 ms); field
+// by field over the interleaved rows, each field's pass fetching the rows
+// again, 17 GB and 5.7 ms (L2 does not hold a resident wave's rows between
+// passes).
 __global__ void __launch_bounds__(kPrtBlock) k_particle_props(const double *__restrict__ coef, int nt, double start,
                                                               double hinv, double *rec, long long n)
 {
-    const long long M = nt + 2, M3 = M * M * M;
+    const long long M = nt + 2;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x; a < n; a += stride) {
         double by[4], dby[4], bx[4], dbx[4], bz[4], dbz[4];
         const int iy = bspline_weights(rec[a], start, hinv, nt, by, dby);
         const int ix = bspline_weights(rec[n + a], start, hinv, nt, bx, dbx);
         const int iz = bspline_weights(rec[2 * n + a], start, hinv, nt, bz, dbz);
-#pragma unroll 1
-        for (int q = 0; q < 5; ++q) {
-            const double *C = coef + q * M3;
-            double v = 0.0, gy = 0.0, gx = 0.0, gz = 0.0;
+        double v[kNF], gy[kNF], gx[kNF], gz[kNF];
 #pragma unroll
-            for (int ia = 0; ia < 4; ++ia) {
-                double va = 0.0, gxa = 0.0, gza = 0.0;
+        for (int q = 0; q < kNF; ++q) v[q] = gy[q] = gx[q] = gz[q] = 0.0;
 #pragma unroll
-                for (int ib = 0; ib < 4; ++ib) {
-                    const double *r = C + ((long long)(iy + ia) * M + (ix + ib)) * M + iz;
-                    const double r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
+        for (int ia = 0; ia < 4; ++ia) {
+            double va[kNF], gxa[kNF], gza[kNF];
+#pragma unroll
+            for (int q = 0; q < kNF; ++q) va[q] = gxa[q] = gza[q] = 0.0;
+#pragma unroll
+            for (int ib = 0; ib < 4; ++ib) {
+                const double *r = coef + (((long long)(iy + ia) * M + (ix + ib)) * M + iz) * kNF;
+                double x[4 * kNF];
+#pragma unroll
+                for (int c = 0; c < 4 * kNF; ++c) x[c] = __ldg(r + c);
+#pragma unroll
+                for (int q = 0; q < kNF; ++q) {
+                    const double r0 = x[q], r1 = x[kNF + q], r2 = x[2 * kNF + q], r3 = x[3 * kNF + q];
                     const double sv = ((bz[0] * r0 + bz[1] * r1) + bz[2] * r2) + bz[3] * r3;
                     const double sd = ((dbz[0] * r0 + dbz[1] * r1) + dbz[2] * r2) + dbz[3] * r3;
-                    va += bx[ib] * sv;
-                    gxa += dbx[ib] * sv;
-                    gza += bx[ib] * sd;
+                    va[q] += bx[ib] * sv;
+                    gxa[q] += dbx[ib] * sv;
+                    gza[q] += bx[ib] * sd;
                 }
-                v += by[ia] * va;
-                gy += dby[ia] * va;
-                gx += by[ia] * gxa;
-                gz += by[ia] * gza;
             }
-            rec[(3 + q) * n + a] = v;
-            rec[(8 + 3 * q) * n + a] = gy * hinv;
-            rec[(9 + 3 * q) * n + a] = gx * hinv;
-            rec[(10 + 3 * q) * n + a] = gz * hinv;
+#pragma unroll
+            for (int q = 0; q < kNF; ++q) {
+                v[q] += by[ia] * va[q];
+                gy[q] += dby[ia] * va[q];
+                gx[q] += by[ia] * gxa[q];
+                gz[q] += by[ia] * gza[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kNF; ++q) {
+            rec[(3 + q) * n + a] = v[q];
+            rec[(8 + 3 * q) * n + a] = gy[q] * hinv;
+            rec[(9 + 3 * q) * n + a] = gx[q] * hinv;
+            rec[(10 + 3 * q) * n + a] = gz[q] * hinv;
         }
     }
 }
@@ -404,9 +437,9 @@ cudaError_t launch_particle_splines(const FieldDev &f, double *coef, const doubl
 {
     const long long nt = f.nc + 6, M = nt + 2;
     k_node_prims<<<grid_for(nt * nt * nt, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(f, coef);
-    k_bspline_zlines<<<grid_for(5 * nt * nt, kZLines, nsm, 6), kZLines, 0, st>>>(coef, nt, w);
-    k_bspline_lines<1><<<grid_for(5 * nt * M, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
-    k_bspline_lines<0><<<grid_for(5 * M * M, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
+    k_bspline_zlines<<<grid_for(kNF * nt * nt, kZThreads, nsm, 4), kZThreads, 0, st>>>(coef, nt, w);
+    k_bspline_lines<1><<<grid_for(kNF * nt * M, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
+    k_bspline_lines<0><<<grid_for(kNF * M * M, kLineBlock, nsm, 16), kLineBlock, 0, st>>>(coef, nt, w);
     return cudaGetLastError();
 }
 
