@@ -22,12 +22,20 @@
 //   --no-field         skip the Results/Field dump
 //   --reinit PATH      write the final state in the Init layout to PATH
 //                      (the reference's WriteReInit targets InitialCondition/, a typo)
+//   --particles        track the particles of InitialConditions/unirand (numparticles
+//                      from particleCount): every step, their properties from the
+//                      current state (generateSplines + getParticleProp) and a move by
+//                      dt (Particle::track) before the field's step, and at every
+//                      statistics line a line "particles t/t0 TKE SijSij SKEWu SKEWw N"
+//                      (GetParticleStats).  The reference defines this tracker
+//                      (update.cpp:1082-1303) but its Evolve never calls it.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <string>
+#include <vector>
 
 #include "gks_driver_io.h"
 
@@ -47,6 +55,7 @@ struct Options {
     int stats_every = 1;
     bool field = true;
     std::string reinit;
+    bool particles = false;
 };
 
 int usage(const char *msg)
@@ -85,6 +94,7 @@ bool parse(int argc, char **argv, Options &o, std::string &err)
         else if (s == "--stats-every") { if (!(v = next("--stats-every"))) return false; o.stats_every = atoi(v); }
         else if (s == "--no-field") o.field = false;
         else if (s == "--reinit") { if (!(v = next("--reinit"))) return false; o.reinit = v; }
+        else if (s == "--particles") o.particles = true;
         else { err = "unknown option " + s; return false; }
     }
     if (!(o.cfl > 0) || o.stats_every < 1) {
@@ -113,6 +123,8 @@ int main(int argc, char **argv)
     if (!(err = gksdrv::read_params(o.casedir, p)).empty()) return usage(err.c_str());
     gksdrv::Field W;
     if (!(err = gksdrv::read_init(o.casedir, p, W)).empty()) return usage(err.c_str());
+    std::vector<double> xyz[3]; // initial particle positions x0, y0, z0
+    if (o.particles && !(err = gksdrv::read_unirand(o.casedir, p, xyz)).empty()) return usage(err.c_str());
 
     const double prandtl = 0.7; // param.h:16
     gksdrv::print_params(p, o.cfl, prandtl);
@@ -142,6 +154,18 @@ int main(int argc, char **argv)
     if ((rc = gks_check(ctx))) return die(ctx, rc, "initial state check");
     double dt = 0;
     if ((rc = gks_timestep(ctx, 0, o.cfl, &dt))) return die(ctx, rc, "timestep");
+    if (o.particles) { // locateParticles (update.cpp:1269-1292) on one rank
+        if ((rc = gks_particles_locate(ctx, 0, p.particles, xyz[0].data(), xyz[1].data(), xyz[2].data())))
+            return die(ctx, rc, "particles_locate");
+    }
+    auto particle_line = [&](double t_over_t0) -> int {
+        gks_particle_stats_out ps;
+        const int r = gks_particles_stats(ctx, 0, &ps);
+        if (!r)
+            printf("particles %.6f %.15e %.15e %.15e %.15e %lld\n", t_over_t0, ps.tke, ps.sijsij, ps.skew_u, ps.skew_w,
+                   ps.count);
+        return r;
+    };
 
     const double tmax = o.tmax_t0 * p.t0;
     double t = 0;
@@ -162,6 +186,11 @@ int main(int argc, char **argv)
                 fprintf(stderr, "gks_dns: %s\n", err.c_str());
             dumped = true;
         }
+        if (o.particles) {
+            if ((rc = gks_particles_props(ctx, 0))) return die(ctx, rc, "particles_props");
+            if (step % o.stats_every == 0 && (rc = particle_line(t / p.t0))) return die(ctx, rc, "particles_stats");
+            if ((rc = gks_particles_track(ctx, 0, dt))) return die(ctx, rc, "particles_track");
+        }
         const auto a = std::chrono::steady_clock::now();
         if ((rc = gks_step(ctx, 1))) return die(ctx, rc, "step");
         if ((rc = gks_sync(ctx))) return die(ctx, rc, "step");
@@ -173,6 +202,10 @@ int main(int argc, char **argv)
     }
     if ((rc = gks_stats(ctx, 0, &st))) return die(ctx, rc, "stats");
     gksdrv::print_stats_line(t / p.t0, st);
+    if (o.particles) {
+        if ((rc = gks_particles_props(ctx, 0))) return die(ctx, rc, "particles_props");
+        if ((rc = particle_line(t / p.t0))) return die(ctx, rc, "particles_stats");
+    }
     if (!o.reinit.empty()) {
         if ((rc = gks_download(ctx, 0, W.ptr))) return die(ctx, rc, "download");
         if (!(err = gksdrv::write_reinit(o.reinit, p, W)).empty()) fprintf(stderr, "gks_dns: %s\n", err.c_str());

@@ -47,6 +47,20 @@ std::string read_params(const std::string &casedir, RunParams &p)
     return "";
 }
 
+std::string read_unirand(const std::string &casedir, const RunParams &p, std::vector<double> xyz[3])
+{
+    const std::string path = casedir + "/InitialConditions/unirand";
+    if (p.particles < 1) return casedir + "/InitialConditions/particleCount holds no particles";
+    std::ifstream in(path, std::ios::binary);
+    if (!in) return "cannot open " + path;
+    for (int q = 0; q < 3; ++q) {
+        xyz[q].resize(p.particles);
+        in.read((char *)xyz[q].data(), p.particles * sizeof(double));
+        if (!in) return path + " is shorter than 3 * numparticles doubles";
+    }
+    return "";
+}
+
 std::string read_init(const std::string &casedir, const RunParams &p, Field &W)
 {
     const std::string path = casedir + "/InitialConditions/Init000";

@@ -38,6 +38,8 @@ struct Field {
 // Returns an empty string on success, else the error message.
 std::string read_params(const std::string &casedir, RunParams &p);
 std::string read_init(const std::string &casedir, const RunParams &p, Field &W);
+// InitialConditions/unirand: x0, y0, z0 of p.particles doubles each (locateParticles, update.cpp:1278-1284).
+std::string read_unirand(const std::string &casedir, const RunParams &p, std::vector<double> xyz[3]);
 std::string write_reinit(const std::string &path, const RunParams &p, const Field &W);
 std::string write_field(const std::string &dir, int rank, int iter, const RunParams &p, const Field &W);
 

@@ -164,17 +164,30 @@ def file_order(a: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()
 
 
-def write_case(casedir: str, case: DhitCase, slab_planes: int | None = None, all_slabs: bool = False) -> None:
-    """Write params, particleCount and Init000.  With slab_planes, the y-slabs
-    of slab_planes planes are the blocks of an (nc/slab_planes) x 1 x 1 process
-    grid: Init000 holds the first slab_planes y-planes (process (0,0,0)) and,
-    with all_slabs, Init<a>00 holds slab a for every process a, the file each
-    rank's Initialize_DHIT reads (FlowField.cpp:73-75)."""
+def particle_positions(n: int, seed: int) -> np.ndarray:
+    """n seeded positions uniform in [0, 2 pi)^3 as (x0, y0, z0), the content of
+    InitialConditions/unirand (read by locateParticles, update.cpp:1278-1284)."""
+    rng = np.random.default_rng(seed)
+    return rng.random((3, n)) * (2.0 * (np.arctan(1.0) * 4.0))
+
+
+def write_case(casedir: str, case: DhitCase, slab_planes: int | None = None, all_slabs: bool = False,
+               particles: int = 0, particle_seed: int = 0) -> None:
+    """Write params, particleCount and Init000 (and, with particles > 0, the
+    particles' initial positions in unirand: x0, y0, z0 of `particles` doubles
+    each).  With slab_planes, the y-slabs of slab_planes planes are the blocks
+    of an (nc/slab_planes) x 1 x 1 process grid: Init000 holds the first
+    slab_planes y-planes (process (0,0,0)) and, with all_slabs, Init<a>00 holds
+    slab a for every process a, the file each rank's Initialize_DHIT reads
+    (FlowField.cpp:73-75)."""
     ic = os.path.join(casedir, "InitialConditions")
     os.makedirs(ic, exist_ok=True)
     write_params(os.path.join(ic, "params"), case)
     with open(os.path.join(ic, "particleCount"), "wb") as f:
-        f.write(struct.pack("<i", 0))
+        f.write(struct.pack("<i", particles))
+    if particles > 0:
+        with open(os.path.join(ic, "unirand"), "wb") as f:
+            f.write(particle_positions(particles, particle_seed).astype("<f8").tobytes())
     if slab_planes and case.nc % slab_planes:
         raise ValueError(f"{slab_planes} planes do not divide nc = {case.nc}")
     nslab = case.nc // slab_planes if (slab_planes and all_slabs) else 1

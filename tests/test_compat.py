@@ -190,3 +190,20 @@ def test_driver_writes_reference_field(tmp_path):
     assert np.array_equal(ijk, rijk)
     scale = np.abs(rvals).max(0)
     assert np.all(np.abs(vals - rvals).max(0) <= 1e-12 * scale), np.abs(vals - rvals).max(0) / scale
+
+
+def test_driver_particles_need_their_inputs(tmp_path):
+    """--particles reads numparticles from particleCount and the positions from
+    unirand; a case without them is refused before any device work."""
+    exe = os.path.join(PKG, "driver", "gks_dns")
+    case = gks_ic.make_dhit(8, seed=2)
+    gks_ic.write_case(str(tmp_path), case)  # particleCount 0, no unirand
+    r = subprocess.run([exe, "--case", str(tmp_path), "--particles"], capture_output=True, text=True)
+    assert r.returncode == 2 and "no particles" in r.stderr
+    gks_ic.write_case(str(tmp_path), case, particles=10)
+    with open(tmp_path / "InitialConditions" / "unirand", "r+b") as f:
+        f.truncate(8 * 25)  # fewer than 3 x 10 doubles
+    r = subprocess.run([exe, "--case", str(tmp_path), "--particles"], capture_output=True, text=True)
+    assert r.returncode == 2 and "shorter" in r.stderr
+    pos = np.fromfile(str(tmp_path / "InitialConditions" / "unirand"))
+    assert pos.size == 25 and np.all((pos >= 0) & (pos < 2 * np.pi))

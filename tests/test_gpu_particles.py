@@ -199,3 +199,36 @@ def test_particles_on_an_ensemble_field_and_after_the_host_step(gks, oracle):
         s.particles_props()
         _, want = oracle_records(oracle, case, host, x0, y0, z0)  # host: the new state, ghosts filled
         assert np.array_equal(s.particles_get(), want)
+
+
+def test_driver_tracks_particles_like_the_oracle(tmp_path, oracle):
+    """gks_dns --particles: every step the particles' properties from the
+    current state, GetParticleStats' line, a move by dt, then the field's
+    step -- the same sequence run by the oracle on the same case."""
+    import os
+    import subprocess
+
+    from conftest import PKG
+
+    nc, n, steps = 16, 400, 3
+    case = gks_ic.make_dhit(nc, k0=4.0, Mt=0.3, Re_lambda=72.0, seed=5)
+    gks_ic.write_case(str(tmp_path), case, particles=n, particle_seed=9)
+    r = subprocess.run([os.path.join(PKG, "driver", "gks_dns"), "--case", str(tmp_path), "--cfl", "0.5", "--steps",
+                        str(steps), "--no-field", "--particles"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = [[float(x) for x in ln.split()[1:]] for ln in r.stdout.splitlines() if ln.startswith("particles ")]
+    assert len(got) == steps + 1
+    _, W = gks_ic.read_init(str(tmp_path))
+    prm = oracle.params(nc, case.gam, case.mu0, case.p0, 1.0, case.Mt, case.t0)
+    dt = 0.5 * prm.dx / oracle.maxval(W, prm)
+    x0, y0, z0 = gks_ic.particle_positions(n, 9)
+    rec = np.zeros((oracle.PREC_FIELDS, n))
+    rec[0], rec[1], rec[2] = y0, x0, z0
+    for s in range(steps + 1):
+        oracle.particle_props(W, prm, rec)
+        st = oracle.particle_stats(rec)
+        want = [st[0], st[1], st[6], st[7], st[8]]
+        np.testing.assert_allclose(got[s][1:], want, rtol=1e-9)
+        if s < steps:
+            oracle.particle_track(rec, dt)
+            oracle.step(W, prm, dt, 1)
