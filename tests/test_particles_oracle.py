@@ -140,3 +140,28 @@ def test_particle_stats_formulas(oracle):
             np.mean(dwdz**3)]
     want += [want[3] / want[2] ** 1.5, want[5] / want[4] ** 1.5, n]
     np.testing.assert_allclose(out, want, rtol=1e-12)
+
+
+def test_bench_particle_cpu_baseline_runs(oracle):
+    """bench.py's particle CPU leg times the oracle on the bench's field: a
+    small case finishes and reports a port on one core."""
+    import os
+    import sys
+
+    from conftest import ROOT
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    case = gks_ic.make_dhit(8, k0=4.0, Mt=0.3, seed=1)
+    W = gks_ic.to_conservative_padded(case)
+    out = bench.particle_cpu_baseline(W, case, 64)
+    assert out["kind"] == "port" and out["cores"] == 1 and out["props_ms"] > 0
+    assert os.path.basename(bench.__file__) == "bench.py"
+
+
+def test_particle_positions_are_seeded_and_in_the_box():
+    a = gks_ic.particle_positions(100, 3)
+    b = gks_ic.particle_positions(100, 3)
+    assert np.array_equal(a, b) and a.shape == (3, 100)
+    assert np.all((a >= 0) & (a < 2 * np.pi))
